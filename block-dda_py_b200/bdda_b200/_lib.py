@@ -1,0 +1,102 @@
+"""ctypes binding of libbdda.so (the C ABI declared in include/bdda.h).
+
+The library is built in-tree by ``block-dda_py_b200/csrc/build.py``.  There is
+no fallback: if the shared object is missing, or no CUDA device is visible,
+every entry point raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+
+import numpy as np
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libbdda.so")
+
+# status codes (include/bdda.h: enum bdda_status)
+OK, NOT_CONVERGED, BREAKDOWN, BAD_ARG, NO_WORKSPACE, TIMEOUT, CUDA_ERROR = range(7)
+# precisions (include/bdda.h: enum bdda_precision)
+C128, C64 = 0, 1
+
+_vp = C.c_void_p
+_sz = C.c_size_t
+_i = C.c_int
+_d = C.c_double
+_pi = C.POINTER(C.c_int)
+
+# name -> (restype, argtypes).  Every symbol of include/bdda.h is listed here;
+# tests check the two lists against each other.
+PROTOTYPES = {
+    "bdda_status_string": (C.c_char_p, [_i]),
+    "bdda_version": (_i, []),
+    "bdda_plan_create": (_i, [_pi, _pi, C.POINTER(_vp)]),
+    "bdda_plan_destroy": (None, [_vp]),
+    "bdda_plan_grid": (_i, [_vp, _pi]),
+    "bdda_plan_radices": (_i, [_vp, _i, _pi, _pi]),
+    "bdda_plan_table_bytes": (_sz, [_vp]),
+    "bdda_plan_attach_tables": (_i, [_vp, _vp, _vp]),
+    "bdda_green_bytes": (_sz, [_vp, _i]),
+    "bdda_green_build_workspace_bytes": (_sz, [_vp]),
+    "bdda_green_build": (_i, [_vp, _d, _d, _vp, _vp, _vp]),
+    "bdda_green_real": (_i, [_vp, _d, _d, _vp, _vp]),
+    "bdda_green_convert": (_i, [_vp, _vp, _vp, _vp]),
+    "bdda_green_export": (_i, [_vp, _vp, _vp, _vp]),
+    "bdda_green_import": (_i, [_vp, _vp, _vp, _vp]),
+    "bdda_mvp_workspace_bytes": (_sz, [_vp, _i, _i]),
+    "bdda_occupancy_map": (_i, [_vp, _vp, _i, _vp, _vp]),
+    "bdda_fft_mvp": (_i, [_vp, _i, _i, _vp, _vp, _vp, _vp, _vp]),
+    "bdda_block_mvp": (_i, [_vp, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+}
+
+
+class BddaError(RuntimeError):
+    """A libbdda call returned a failure status."""
+
+    def __init__(self, status: int, where: str):
+        self.status = status
+        super().__init__("%s: %s (status %d)" % (where, status_string(status), status))
+
+
+_lock = threading.Lock()
+_lib = None
+
+
+def load() -> C.CDLL:
+    """Load libbdda.so once and bind the prototypes; raise if it is absent."""
+    global _lib
+    with _lock:
+        if _lib is None:
+            if not os.path.exists(LIB_PATH):
+                raise ImportError(
+                    "libbdda.so not found at %s; build it with "
+                    "`python block-dda_py_b200/csrc/build.py`" % LIB_PATH)
+            lib = C.CDLL(LIB_PATH)
+            for name, (res, args) in PROTOTYPES.items():
+                fn = getattr(lib, name)
+                fn.restype = res
+                fn.argtypes = args
+            _lib = lib
+    return _lib
+
+
+def status_string(status: int) -> str:
+    return load().bdda_status_string(status).decode()
+
+
+def check(status: int, where: str) -> int:
+    """Raise for any status other than OK / NOT_CONVERGED."""
+    if status in (OK, NOT_CONVERGED):
+        return status
+    if status == BAD_ARG:
+        raise ValueError("%s: %s" % (where, status_string(status)))
+    if status == BREAKDOWN:
+        raise np.linalg.LinAlgError("%s: %s" % (where, status_string(status)))
+    raise BddaError(status, where)
+
+
+def int3(values) -> C.Array:
+    arr = (C.c_int * 3)()
+    for i, v in enumerate(values):
+        arr[i] = int(v)
+    return arr

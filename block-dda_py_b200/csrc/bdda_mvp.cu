@@ -1,0 +1,654 @@
+// Doubled-grid FFT matrix-vector product of block-DDA on sm_100a.
+//
+// One block MVP is five pencil passes over a field buffer F of shape
+// (Nx, My, Mz, 3L) (x natural; y, z spectra in digit-reversed order):
+//   Z   : gather S through the occupancy map, forward z-FFT   (Nx*Ny pencils)
+//   Y   : forward y-FFT, Ny rows in, My out                    (Nx*Mz pencils)
+//   X   : forward x-FFT, 3x3 symmetric Green multiply, inverse (My*Mz pencils)
+//   Y^-1: inverse y-FFT, My rows in, Ny out                    (Nx*Mz pencils)
+//   Z^-1: inverse z-FFT, crop, diagonal + Jacobi epilogue, scatter back
+// which is the reference's pad -> fftn -> Au_til @ P~ -> ifftn -> crop ->
+// gather (mvp_fft/mvp_fft.py:151-169, bl_krylov/bl_krylov.py:47-55) with
+// the zero rows never read and the rows that are cropped never written.
+#include <climits>
+#include <cmath>
+#include <cstring>
+#include <type_traits>
+
+#include "bdda_internal.h"
+
+namespace bdda {
+
+enum PassKind { K_FWD = 0, K_FWD_GATHER = 1, K_GREEN_Z = 2, K_CONV = 3, K_INV = 4, K_INV_SCATTER = 5 };
+
+struct PassArgs {
+  AxisFFT ax;
+  int n_in, n_out;      // rows read (the rest are zero) / rows written
+  int P1;               // pencil index p = p0 * P1 + p1
+  int ntile;            // column tiles per pencil
+  int L;                // right-hand sides
+  int64_t C;            // complex values per grid row (3L)
+  int64_t src_p0, src_p1, src_row;
+  int64_t dst_p0, dst_p1, dst_row;
+  const void* src;
+  void* dst;
+  const void* tw;       // this axis' twiddles, M entries
+  const int32_t* cell_map;
+  int64_t cell_p0, cell_p1;
+  const void* S;
+  const void* diag;
+  const void* jpre;
+  double scale;
+  const void* ghat;
+  int gN[3], gM[3];
+  double lf, k;
+};
+
+__device__ __forceinline__ bool axis_disp(int I, int N, int M, int& d) {
+  if (I <= N - 1) { d = I; return true; }
+  if (I >= M - (N - 1)) { d = I - M; return true; }
+  d = 0;
+  return false;
+}
+
+// Six unique components of A'(r) at cyclic index (ix, iy, iz)
+// (mvp_fft/mvp_fft.py:49-92 with the displacement map generalised to M >= 2N-1).
+__device__ void green_row(const PassArgs& a, int ix, int iy, int iz, double2* out) {
+  int dx, dy, dz;
+  const bool ok = axis_disp(ix, a.gN[0], a.gM[0], dx) & axis_disp(iy, a.gN[1], a.gM[1], dy) &
+                  axis_disp(iz, a.gN[2], a.gM[2], dz);
+  if (!ok || (dx == 0 && dy == 0 && dz == 0)) {
+    for (int c = 0; c < 6; ++c) out[c] = make_double2(0.0, 0.0);
+    return;
+  }
+  const double X = dx * a.lf, Y = dy * a.lf, Z = dz * a.lf;
+  const double r = sqrt(X * X + Y * Y + Z * Z);
+  const double u[3] = {X / r, Y / r, Z / r};
+  double sn, cs;
+  sincos(a.k * r, &sn, &cs);
+  const double pr = cs / r, pim = sn / r;            // e^{ikr} / r
+  const double nr = 1.0 / (r * r), ni = -a.k / r;    // (1 - ikr) / r^2
+  const double k2 = a.k * a.k;
+  const int ia[6] = {0, 0, 0, 1, 1, 2}, ib[6] = {0, 1, 2, 1, 2, 2};
+#pragma unroll
+  for (int c = 0; c < 6; ++c) {
+    const double uu = u[ia[c]] * u[ib[c]];
+    const double delta = (ia[c] == ib[c]) ? 1.0 : 0.0;
+    const double q = delta - 3.0 * uu;
+    const double tr = k2 * (uu - delta) + nr * q, ti = ni * q;
+    out[c] = make_double2(pr * tr - pim * ti, pr * ti + pim * tr);
+  }
+}
+
+template <typename T, int KIND, int LT>
+__global__ void __launch_bounds__(256) pencil_kernel(const PassArgs a) {
+  constexpr int W = 3 * LT;
+  typedef typename real_of<T>::type F;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const int M = a.ax.M;
+  T* tw = reinterpret_cast<T*>(smraw);
+  T* sm = tw + M;
+  const int tile = blockIdx.x % a.ntile;
+  const int64_t p = blockIdx.x / a.ntile;
+  const int64_t p0 = p / a.P1, p1 = p - p0 * a.P1;
+
+  const T* twg = static_cast<const T*>(a.tw);
+  for (int i = threadIdx.x; i < M; i += blockDim.x) tw[i] = twg[i];
+
+  // ---- load one pencil x tile into shared memory (zero beyond n_in) ----
+  if constexpr (KIND == K_GREEN_Z) {
+    if constexpr (std::is_same<T, double2>::value) {
+      for (int i = threadIdx.x; i < M; i += blockDim.x) green_row(a, (int)p0, (int)p1, i, sm + i * W);
+    }
+  } else {
+    const T* src = static_cast<const T*>((KIND == K_FWD_GATHER && a.cell_map) ? a.S : a.src);
+    const int64_t base = p0 * a.src_p0 + p1 * a.src_p1;
+    const int total = M * W;
+    constexpr int U = 4;
+    for (int e0 = threadIdx.x; e0 < total; e0 += U * blockDim.x) {
+      T v[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int e = e0 + u * blockDim.x;
+        const int i = e / W, c = e - i * W;
+        const int comp = c / LT, l = tile * LT + (c - comp * LT);
+        v[u] = mkc<T>(F(0), F(0));
+        if (e < total && i < a.n_in && l < a.L) {
+          const int64_t gcol = (int64_t)comp * a.L + l;
+          if constexpr (KIND == K_FWD_GATHER) {
+            const int64_t cell = p0 * a.cell_p0 + p1 * a.cell_p1 + i;
+            if (a.cell_map) {
+              const int m = a.cell_map[cell];
+              if (m >= 0) v[u] = src[(int64_t)m * a.C + gcol];
+            } else {
+              v[u] = src[cell * a.C + gcol];
+            }
+          } else {
+            v[u] = src[base + (int64_t)i * a.src_row + gcol];
+          }
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int e = e0 + u * blockDim.x;
+        if (e < total) sm[e] = v[u];
+      }
+    }
+  }
+  __syncthreads();
+
+  // ---- transform ----
+  if constexpr (KIND == K_INV || KIND == K_INV_SCATTER) {
+    fft_stages<true, W>(sm, tw, a.ax);
+  } else {
+    fft_stages<false, W>(sm, tw, a.ax);
+  }
+
+  if constexpr (KIND == K_CONV) {
+    // per-frequency y = G v with G complex symmetric: the 6 unique entries of
+    // this x-pencil are read once for all LT right-hand sides of the tile
+    const T* g = static_cast<const T*>(a.ghat) + p * (int64_t)M * 6;
+    for (int job = threadIdx.x; job < M * LT; job += blockDim.x) {
+      const int px = job / LT, li = job - px * LT;
+      T* r = sm + px * W + li;
+      const T v0 = r[0], v1 = r[LT], v2 = r[2 * LT];
+      const T* gp = g + px * 6;
+      const T gxx = gp[0], gxy = gp[1], gxz = gp[2], gyy = gp[3], gyz = gp[4], gzz = gp[5];
+      r[0] = cadd(cadd(cmul(gxx, v0), cmul(gxy, v1)), cmul(gxz, v2));
+      r[LT] = cadd(cadd(cmul(gxy, v0), cmul(gyy, v1)), cmul(gyz, v2));
+      r[2 * LT] = cadd(cadd(cmul(gxz, v0), cmul(gyz, v1)), cmul(gzz, v2));
+    }
+    __syncthreads();
+    fft_stages<true, W>(sm, tw, a.ax);
+  }
+
+  // ---- store n_out rows ----
+  const int total = a.n_out * W;
+  for (int e = threadIdx.x; e < total; e += blockDim.x) {
+    const int i = e / W, c = e - i * W;
+    const int comp = c / LT, l = tile * LT + (c - comp * LT);
+    if (l >= a.L) continue;
+    const int64_t gcol = (int64_t)comp * a.L + l;
+    const T v = sm[e];
+    if constexpr (KIND == K_INV_SCATTER) {
+      const int64_t cell = p0 * a.cell_p0 + p1 * a.cell_p1 + i;
+      const F sc = F(a.scale);
+      T* out = static_cast<T*>(a.dst);
+      if (a.cell_map) {
+        const int m = a.cell_map[cell];
+        if (m >= 0) {
+          const int64_t row = 3 * (int64_t)m + comp;
+          const int64_t idx = (int64_t)m * a.C + gcol;
+          const T d = static_cast<const T*>(a.diag)[row];
+          const T j = static_cast<const T*>(a.jpre)[row];
+          const T s = static_cast<const T*>(a.S)[idx];
+          out[idx] = cmul(cadd(cmul(d, s), cscale(v, sc)), j);
+        }
+      } else {
+        out[cell * a.C + gcol] = cscale(v, sc);
+      }
+    } else {
+      static_cast<T*>(a.dst)[p0 * a.dst_p0 + p1 * a.dst_p1 + (int64_t)i * a.dst_row + gcol] = v;
+    }
+  }
+}
+
+// Shared-memory budget per CTA for the pencil tiles; tiles are chosen as wide
+// as fit (at most 3 CTAs per SM at the default).
+static size_t g_tile_smem_budget = 72 * 1024;
+
+static int pick_lt(int M, int L, size_t esz) {
+  const int cand[4] = {8, 4, 2, 1};
+  for (int lt : cand) {
+    if (lt > 1 && lt / 2 >= L) continue;
+    if ((size_t)M * (1 + 3 * lt) * esz <= g_tile_smem_budget) return lt;
+  }
+  return 1;
+}
+
+template <typename T, int KIND, int LT>
+static int launch_lt(PassArgs a, int64_t P0, cudaStream_t st) {
+  auto kern = pencil_kernel<T, KIND, LT>;
+  a.ntile = (a.L + LT - 1) / LT;
+  const size_t smem = (size_t)a.ax.M * (1 + 3 * LT) * sizeof(T);
+  if (smem > 227 * 1024) return BDDA_BAD_ARG;
+  const int64_t nblk = P0 * a.P1 * a.ntile;
+  if (nblk <= 0) return BDDA_OK;
+  if (nblk > INT_MAX) return BDDA_BAD_ARG;
+  BDDA_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  kern<<<(unsigned)nblk, 256, smem, st>>>(a);
+  BDDA_CUDA_TRY(cudaGetLastError());
+  return BDDA_OK;
+}
+
+template <typename T, int KIND>
+static int launch_pass(const PassArgs& a, int64_t P0, int lt, cudaStream_t st) {
+  switch (lt) {
+    case 8: return launch_lt<T, KIND, 8>(a, P0, st);
+    case 4: return launch_lt<T, KIND, 4>(a, P0, st);
+    case 2: return launch_lt<T, KIND, 2>(a, P0, st);
+    default: return launch_lt<T, KIND, 1>(a, P0, st);
+  }
+}
+
+template <typename T> struct TwOff;
+template <> struct TwOff<double2> { static size_t get(const bdda_plan* p, int ax) { return p->tw64_off[ax]; } };
+template <> struct TwOff<float2> { static size_t get(const bdda_plan* p, int ax) { return p->tw32_off[ax]; } };
+
+#define BDDA_TRY(expr)               \
+  do {                               \
+    int s_ = (expr);                 \
+    if (s_ != BDDA_OK) return s_;    \
+  } while (0)
+
+// The five passes.  cell_map == nullptr: dense cuboid in and out, no epilogue
+// (fft_mvp); otherwise the sparse block MVP with diagonal and Jacobi scaling.
+template <typename T>
+static int run_mvp(const bdda_plan* plan, int L, const T* ghat, const int32_t* cell_map,
+                   const T* src, const T* diag, const T* jpre, T* out, T* F, cudaStream_t st) {
+  const int64_t Nx = plan->n[0], Ny = plan->n[1], Nz = plan->n[2];
+  const int64_t Mx = plan->ax[0].M, My = plan->ax[1].M, Mz = plan->ax[2].M;
+  const int64_t C = 3 * (int64_t)L;
+  PassArgs b;
+  memset(&b, 0, sizeof(b));
+  b.L = L;
+  b.C = C;
+
+  {  // Z: gather + forward z
+    PassArgs a = b;
+    a.ax = plan->ax[2]; a.tw = table_ptr<T>(plan, TwOff<T>::get(plan, 2));
+    a.n_in = (int)Nz; a.n_out = (int)Mz; a.P1 = (int)Ny;
+    a.cell_map = cell_map; a.cell_p0 = Ny * Nz; a.cell_p1 = Nz;
+    a.S = src; a.src = src;
+    a.dst = F; a.dst_p0 = My * Mz * C; a.dst_p1 = Mz * C; a.dst_row = C;
+    BDDA_TRY((launch_pass<T, K_FWD_GATHER>(a, Nx, pick_lt((int)Mz, L, sizeof(T)), st)));
+  }
+  PassArgs ay = b;  // Y and Y^-1 share the pencil geometry
+  ay.ax = plan->ax[1]; ay.tw = table_ptr<T>(plan, TwOff<T>::get(plan, 1));
+  ay.P1 = (int)Mz; ay.src = F; ay.dst = F;
+  ay.src_p0 = ay.dst_p0 = My * Mz * C; ay.src_p1 = ay.dst_p1 = C; ay.src_row = ay.dst_row = Mz * C;
+  const int lty = pick_lt((int)My, L, sizeof(T));
+  {
+    PassArgs a = ay;
+    a.n_in = (int)Ny; a.n_out = (int)My;
+    BDDA_TRY((launch_pass<T, K_FWD>(a, Nx, lty, st)));
+  }
+  {  // X: forward, Green multiply, inverse
+    PassArgs a = b;
+    a.ax = plan->ax[0]; a.tw = table_ptr<T>(plan, TwOff<T>::get(plan, 0));
+    a.n_in = (int)Nx; a.n_out = (int)Nx; a.P1 = (int)Mz;
+    a.src = F; a.dst = F;
+    a.src_p0 = a.dst_p0 = Mz * C; a.src_p1 = a.dst_p1 = C; a.src_row = a.dst_row = My * Mz * C;
+    a.ghat = ghat;
+    BDDA_TRY((launch_pass<T, K_CONV>(a, My, pick_lt((int)Mx, L, sizeof(T)), st)));
+  }
+  {
+    PassArgs a = ay;
+    a.n_in = (int)My; a.n_out = (int)Ny;
+    BDDA_TRY((launch_pass<T, K_INV>(a, Nx, lty, st)));
+  }
+  {  // Z^-1 + crop + epilogue
+    PassArgs a = b;
+    a.ax = plan->ax[2]; a.tw = table_ptr<T>(plan, TwOff<T>::get(plan, 2));
+    a.n_in = (int)Mz; a.n_out = (int)Nz; a.P1 = (int)Ny;
+    a.src = F; a.src_p0 = My * Mz * C; a.src_p1 = Mz * C; a.src_row = C;
+    a.cell_map = cell_map; a.cell_p0 = Ny * Nz; a.cell_p1 = Nz;
+    a.S = src; a.diag = diag; a.jpre = jpre; a.dst = out;
+    a.scale = 1.0 / (double)(Mx * My * Mz);
+    BDDA_TRY((launch_pass<T, K_INV_SCATTER>(a, Nx, pick_lt((int)Mz, L, sizeof(T)), st)));
+  }
+  return BDDA_OK;
+}
+
+template <typename T>
+int block_mvp_impl(const bdda_plan* plan, int L, const T* ghat, const int32_t* cell_map,
+                   const T* diag, const T* jpre, const T* S, T* out, T* work, cudaStream_t st) {
+  return run_mvp<T>(plan, L, ghat, cell_map, S, diag, jpre, out, work, st);
+}
+template int block_mvp_impl<double2>(const bdda_plan*, int, const double2*, const int32_t*,
+                                     const double2*, const double2*, const double2*, double2*,
+                                     double2*, cudaStream_t);
+template int block_mvp_impl<float2>(const bdda_plan*, int, const float2*, const int32_t*,
+                                    const float2*, const float2*, const float2*, float2*, float2*,
+                                    cudaStream_t);
+
+// ---- small helper kernels ----------------------------------------------------
+__global__ void occupancy_kernel(const int64_t* address, int n_occ, int64_t nc, int32_t* cell_map) {
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m < n_occ) {
+    const int64_t cell = address[m];
+    if (cell >= 0 && cell < nc) cell_map[cell] = m;
+  }
+}
+
+__global__ void convert_kernel(const double2* in, float2* out, int64_t n) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = make_float2((float)in[i].x, (float)in[i].y);
+}
+
+// Real-space A'(r) in natural order, (Mx, My, Mz, 3, 3) (mvp_fft/mvp_fft.py:13-94).
+__global__ void green_real_kernel(PassArgs a, double2* out) {
+  const int64_t total = (int64_t)a.gM[0] * a.gM[1] * a.gM[2];
+  const int ia[6] = {0, 0, 0, 1, 1, 2}, ib[6] = {0, 1, 2, 1, 2, 2};
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int iz = (int)(t % a.gM[2]);
+    const int64_t q = t / a.gM[2];
+    const int iy = (int)(q % a.gM[1]);
+    const int ix = (int)(q / a.gM[1]);
+    double2 g[6];
+    green_row(a, ix, iy, iz, g);
+    for (int c = 0; c < 6; ++c) {
+      out[t * 9 + ia[c] * 3 + ib[c]] = g[c];
+      out[t * 9 + ib[c] * 3 + ia[c]] = g[c];
+    }
+  }
+}
+
+struct GreenMap {
+  int M[3];
+  const int32_t* rev[3];
+};
+
+// library order [(py*Mz + pz)*Mx + px][6]  <->  natural (kx, ky, kz, 3, 3)
+template <bool EXPORT>
+__global__ void green_reorder_kernel(GreenMap g, const double2* in, double2* out) {
+  const int64_t total = (int64_t)g.M[0] * g.M[1] * g.M[2];
+  const int ia[6] = {0, 0, 0, 1, 1, 2}, ib[6] = {0, 1, 2, 1, 2, 2};
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int px = (int)(t % g.M[0]);
+    const int64_t q = t / g.M[0];
+    const int pz = (int)(q % g.M[2]);
+    const int py = (int)(q / g.M[2]);
+    const int64_t nat = ((int64_t)g.rev[0][px] * g.M[1] + g.rev[1][py]) * g.M[2] + g.rev[2][pz];
+    for (int c = 0; c < 6; ++c) {
+      if (EXPORT) {
+        const double2 v = in[t * 6 + c];
+        out[nat * 9 + ia[c] * 3 + ib[c]] = v;
+        out[nat * 9 + ib[c] * 3 + ia[c]] = v;
+      } else {
+        out[t * 6 + c] = in[nat * 9 + ia[c] * 3 + ib[c]];
+      }
+    }
+  }
+}
+
+static bool smooth7(int m) {
+  for (int p : {2, 3, 5, 7})
+    while (m % p == 0) m /= p;
+  return m == 1;
+}
+
+static int factor_axis(int M, AxisFFT& ax) {
+  int m = M, ns = 0;
+  int r[kMaxStages];
+  while (m % 8 == 0 && ns < kMaxStages) { r[ns++] = 8; m /= 8; }
+  if (m % 4 == 0 && ns < kMaxStages) { r[ns++] = 4; m /= 4; }
+  if (m % 2 == 0 && ns < kMaxStages) { r[ns++] = 2; m /= 2; }
+  for (int p : {3, 5, 7})
+    while (m % p == 0 && ns < kMaxStages) { r[ns++] = p; m /= p; }
+  if (m != 1) return BDDA_BAD_ARG;
+  ax.M = M;
+  ax.nst = ns;
+  int B = M;
+  for (int s = 0; s < ns; ++s) { ax.rad[s] = r[s]; ax.blk[s] = B; B /= r[s]; }
+  for (int s = ns; s < kMaxStages; ++s) { ax.rad[s] = 1; ax.blk[s] = 1; }
+  return BDDA_OK;
+}
+
+}  // namespace bdda
+
+using namespace bdda;
+
+static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+extern "C" {
+
+const char* bdda_status_string(int s) {
+  switch (s) {
+    case BDDA_OK: return "ok";
+    case BDDA_NOT_CONVERGED: return "not converged";
+    case BDDA_BREAKDOWN: return "breakdown: singular or non-finite small system";
+    case BDDA_BAD_ARG: return "bad argument";
+    case BDDA_NO_WORKSPACE: return "workspace or plan tables missing";
+    case BDDA_TIMEOUT: return "device wait timed out";
+    case BDDA_CUDA_ERROR: return "CUDA runtime error";
+    default: return "unknown status";
+  }
+}
+
+int bdda_version(void) { return 100; }
+
+int bdda_plan_create(const int n[3], const int m[3], bdda_plan** out) {
+  if (!n || !out) return BDDA_BAD_ARG;
+  bdda_plan* p = new bdda_plan();
+  p->dev_tables = nullptr;
+  for (int a = 0; a < 3; ++a) {
+    if (n[a] < 1 || n[a] > 16384) { delete p; return BDDA_BAD_ARG; }
+    p->n[a] = n[a];
+    int M;
+    if (m) {
+      M = m[a];
+      if (M < 2 * n[a] - 1 || !smooth7(M)) { delete p; return BDDA_BAD_ARG; }
+    } else {
+      M = 2 * n[a];
+      while (!smooth7(M)) M += 2;
+    }
+    if (factor_axis(M, p->ax[a]) != BDDA_OK) { delete p; return BDDA_BAD_ARG; }
+  }
+  // device tables: twiddles (both precisions) and position -> frequency maps
+  size_t off = 0;
+  for (int a = 0; a < 3; ++a) {
+    const int M = p->ax[a].M;
+    p->tw64_off[a] = off; off = align256(off + (size_t)M * sizeof(double2));
+    p->tw32_off[a] = off; off = align256(off + (size_t)M * sizeof(float2));
+    p->rev_off[a] = off;  off = align256(off + (size_t)M * sizeof(int32_t));
+  }
+  p->table_bytes = off;
+  p->host_tables.assign(off, 0);
+  for (int a = 0; a < 3; ++a) {
+    const AxisFFT& ax = p->ax[a];
+    const int M = ax.M;
+    double2* t64 = reinterpret_cast<double2*>(p->host_tables.data() + p->tw64_off[a]);
+    float2* t32 = reinterpret_cast<float2*>(p->host_tables.data() + p->tw32_off[a]);
+    int32_t* rev = reinterpret_cast<int32_t*>(p->host_tables.data() + p->rev_off[a]);
+    const long double twopi = 6.283185307179586476925286766559005768L;
+    for (int k = 0; k < M; ++k) {
+      const long double ang = twopi * (long double)k / (long double)M;
+      const double c = (double)cosl(ang), s = -(double)sinl(ang);
+      t64[k] = make_double2(c, s);
+      t32[k] = make_float2((float)c, (float)s);
+      // digit reversal of the DIF stage order: position digits (q0 q1 ...)
+      // with position = q0*blk1 + q1*blk2 + ..., frequency = q0 + r0*(q1 + r1*(...))
+      int rem = k, mult = 1, f = 0;
+      for (int s2 = 0; s2 < ax.nst; ++s2) {
+        const int span = ax.blk[s2] / ax.rad[s2];
+        const int q = rem / span;
+        rem -= q * span;
+        f += q * mult;
+        mult *= ax.rad[s2];
+      }
+      rev[k] = f;
+    }
+  }
+  *out = p;
+  return BDDA_OK;
+}
+
+void bdda_plan_destroy(bdda_plan* p) { delete p; }
+
+int bdda_plan_grid(const bdda_plan* p, int m[3]) {
+  if (!p || !m) return BDDA_BAD_ARG;
+  for (int a = 0; a < 3; ++a) m[a] = p->ax[a].M;
+  return BDDA_OK;
+}
+
+int bdda_plan_radices(const bdda_plan* p, int axis, int radices[12], int* nstage) {
+  if (!p || axis < 0 || axis > 2 || !radices || !nstage) return BDDA_BAD_ARG;
+  *nstage = p->ax[axis].nst;
+  for (int s = 0; s < kMaxStages; ++s) radices[s] = s < p->ax[axis].nst ? p->ax[axis].rad[s] : 0;
+  return BDDA_OK;
+}
+
+size_t bdda_plan_table_bytes(const bdda_plan* p) { return p ? p->table_bytes : 0; }
+
+int bdda_plan_attach_tables(bdda_plan* p, void* dev, void* stream) {
+  if (!p || !dev) return BDDA_BAD_ARG;
+  BDDA_CUDA_TRY(cudaMemcpyAsync(dev, p->host_tables.data(), p->table_bytes, cudaMemcpyHostToDevice,
+                                (cudaStream_t)stream));
+  // the host copy must not change before the upload completes
+  BDDA_CUDA_TRY(cudaStreamSynchronize((cudaStream_t)stream));
+  p->dev_tables = dev;
+  return BDDA_OK;
+}
+
+size_t bdda_green_bytes(const bdda_plan* p, int prec) {
+  return p ? (size_t)grid_points(p) * 6 * cplx_bytes(prec) : 0;
+}
+
+size_t bdda_green_build_workspace_bytes(const bdda_plan* p) {
+  return p ? (size_t)grid_points(p) * 6 * sizeof(double2) : 0;
+}
+
+int bdda_green_build(const bdda_plan* p, double lf, double k, void* ghat, void* work, void* stream) {
+  if (!p || !ghat) return BDDA_BAD_ARG;
+  if (!work || !p->dev_tables) return BDDA_NO_WORKSPACE;
+  if (!(lf > 0.0) || !std::isfinite(k)) return BDDA_BAD_ARG;
+  cudaStream_t st = (cudaStream_t)stream;
+  const int64_t Mx = p->ax[0].M, My = p->ax[1].M, Mz = p->ax[2].M;
+  double2* G = static_cast<double2*>(work);
+  PassArgs b;
+  memset(&b, 0, sizeof(b));
+  b.L = 2;   // 6 components = 3 "components" x 2 columns: the tile mapping is the identity
+  b.C = 6;
+  for (int a = 0; a < 3; ++a) { b.gN[a] = p->n[a]; b.gM[a] = p->ax[a].M; }
+  b.lf = lf;
+  b.k = k;
+  {  // real-space tensor evaluated on the fly, forward z
+    PassArgs a = b;
+    a.ax = p->ax[2]; a.tw = table_ptr<double2>(p, p->tw64_off[2]);
+    a.n_in = a.n_out = (int)Mz; a.P1 = (int)My;
+    a.dst = G; a.dst_p0 = My * Mz * 6; a.dst_p1 = Mz * 6; a.dst_row = 6;
+    BDDA_TRY((launch_lt<double2, K_GREEN_Z, 2>(a, Mx, st)));
+  }
+  {  // forward y
+    PassArgs a = b;
+    a.ax = p->ax[1]; a.tw = table_ptr<double2>(p, p->tw64_off[1]);
+    a.n_in = a.n_out = (int)My; a.P1 = (int)Mz;
+    a.src = G; a.dst = G;
+    a.src_p0 = a.dst_p0 = My * Mz * 6; a.src_p1 = a.dst_p1 = 6; a.src_row = a.dst_row = Mz * 6;
+    BDDA_TRY((launch_lt<double2, K_FWD, 2>(a, Mx, st)));
+  }
+  {  // forward x into the x-pencil-major spectrum
+    PassArgs a = b;
+    a.ax = p->ax[0]; a.tw = table_ptr<double2>(p, p->tw64_off[0]);
+    a.n_in = a.n_out = (int)Mx; a.P1 = (int)Mz;
+    a.src = G; a.src_p0 = Mz * 6; a.src_p1 = 6; a.src_row = My * Mz * 6;
+    a.dst = ghat; a.dst_p0 = Mz * Mx * 6; a.dst_p1 = Mx * 6; a.dst_row = 6;
+    BDDA_TRY((launch_lt<double2, K_FWD, 2>(a, My, st)));
+  }
+  return BDDA_OK;
+}
+
+int bdda_green_real(const bdda_plan* p, double lf, double k, void* full, void* stream) {
+  if (!p || !full || !(lf > 0.0) || !std::isfinite(k)) return BDDA_BAD_ARG;
+  PassArgs a;
+  memset(&a, 0, sizeof(a));
+  for (int d = 0; d < 3; ++d) { a.gN[d] = p->n[d]; a.gM[d] = p->ax[d].M; }
+  a.lf = lf;
+  a.k = k;
+  green_real_kernel<<<148 * 8, 256, 0, (cudaStream_t)stream>>>(a, static_cast<double2*>(full));
+  BDDA_CUDA_TRY(cudaGetLastError());
+  return BDDA_OK;
+}
+
+int bdda_green_convert(const bdda_plan* p, const void* g64, void* g32, void* stream) {
+  if (!p || !g64 || !g32) return BDDA_BAD_ARG;
+  const int64_t n = grid_points(p) * 6;
+  convert_kernel<<<148 * 8, 256, 0, (cudaStream_t)stream>>>(static_cast<const double2*>(g64),
+                                                            static_cast<float2*>(g32), n);
+  BDDA_CUDA_TRY(cudaGetLastError());
+  return BDDA_OK;
+}
+
+static int green_reorder(const bdda_plan* p, const void* in, void* out, void* stream, bool exp) {
+  if (!p || !in || !out) return BDDA_BAD_ARG;
+  if (!p->dev_tables) return BDDA_NO_WORKSPACE;
+  GreenMap g;
+  for (int a = 0; a < 3; ++a) {
+    g.M[a] = p->ax[a].M;
+    g.rev[a] = table_ptr<int32_t>(p, p->rev_off[a]);
+  }
+  if (exp)
+    green_reorder_kernel<true><<<148 * 8, 256, 0, (cudaStream_t)stream>>>(
+        g, static_cast<const double2*>(in), static_cast<double2*>(out));
+  else
+    green_reorder_kernel<false><<<148 * 8, 256, 0, (cudaStream_t)stream>>>(
+        g, static_cast<const double2*>(in), static_cast<double2*>(out));
+  BDDA_CUDA_TRY(cudaGetLastError());
+  return BDDA_OK;
+}
+
+int bdda_green_export(const bdda_plan* p, const void* ghat, void* full, void* stream) {
+  return green_reorder(p, ghat, full, stream, true);
+}
+
+int bdda_green_import(const bdda_plan* p, const void* full, void* ghat, void* stream) {
+  return green_reorder(p, full, ghat, stream, false);
+}
+
+size_t bdda_mvp_workspace_bytes(const bdda_plan* p, int prec, int L) {
+  if (!p || L < 1) return 0;
+  return (size_t)p->n[0] * p->ax[1].M * p->ax[2].M * 3 * (size_t)L * cplx_bytes(prec);
+}
+
+int bdda_occupancy_map(const bdda_plan* p, const int64_t* address, int n_occ, int32_t* cell_map,
+                       void* stream) {
+  if (!p || !cell_map || n_occ < 0 || (n_occ > 0 && !address)) return BDDA_BAD_ARG;
+  cudaStream_t st = (cudaStream_t)stream;
+  const int64_t nc = cells(p);
+  BDDA_CUDA_TRY(cudaMemsetAsync(cell_map, 0xff, (size_t)nc * sizeof(int32_t), st));
+  if (n_occ > 0) {
+    occupancy_kernel<<<(n_occ + 255) / 256, 256, 0, st>>>(address, n_occ, nc, cell_map);
+    BDDA_CUDA_TRY(cudaGetLastError());
+  }
+  return BDDA_OK;
+}
+
+int bdda_fft_mvp(const bdda_plan* p, int prec, int L, const void* ghat, const void* P_full,
+                 void* Y_full, void* work, void* stream) {
+  if (!p || L < 1 || !ghat || !P_full || !Y_full) return BDDA_BAD_ARG;
+  if (!work || !p->dev_tables) return BDDA_NO_WORKSPACE;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (prec == BDDA_C128)
+    return run_mvp<double2>(p, L, static_cast<const double2*>(ghat), nullptr,
+                            static_cast<const double2*>(P_full), nullptr, nullptr,
+                            static_cast<double2*>(Y_full), static_cast<double2*>(work), st);
+  if (prec == BDDA_C64)
+    return run_mvp<float2>(p, L, static_cast<const float2*>(ghat), nullptr,
+                           static_cast<const float2*>(P_full), nullptr, nullptr,
+                           static_cast<float2*>(Y_full), static_cast<float2*>(work), st);
+  return BDDA_BAD_ARG;
+}
+
+int bdda_block_mvp(const bdda_plan* p, int prec, int L, const void* ghat, const int32_t* cell_map,
+                   const void* diag, const void* jpre, const void* S, void* out, void* work,
+                   void* stream) {
+  if (!p || L < 1 || !ghat || !cell_map || !diag || !jpre || !S || !out) return BDDA_BAD_ARG;
+  if (!work || !p->dev_tables) return BDDA_NO_WORKSPACE;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (prec == BDDA_C128)
+    return block_mvp_impl<double2>(p, L, static_cast<const double2*>(ghat), cell_map,
+                                   static_cast<const double2*>(diag), static_cast<const double2*>(jpre),
+                                   static_cast<const double2*>(S), static_cast<double2*>(out),
+                                   static_cast<double2*>(work), st);
+  if (prec == BDDA_C64)
+    return block_mvp_impl<float2>(p, L, static_cast<const float2*>(ghat), cell_map,
+                                  static_cast<const float2*>(diag), static_cast<const float2*>(jpre),
+                                  static_cast<const float2*>(S), static_cast<float2*>(out),
+                                  static_cast<float2*>(work), st);
+  return BDDA_BAD_ARG;
+}
+
+}  // extern "C"

@@ -1,0 +1,115 @@
+/*
+ * bdda.h -- C ABI of libbdda.so, the B200 (sm_100a) hot path of block-DDA:
+ * the Goodman doubled-grid FFT matrix-vector product and the block Krylov
+ * solvers built on it.
+ *
+ * Conventions
+ *  - Every device buffer is allocated by the caller; the library never
+ *    allocates or frees device memory.  Sizes come from the *_bytes queries.
+ *  - All calls are stream-ordered on the given stream (a cudaStream_t passed
+ *    as void*; NULL = legacy default stream).  Solver entry points read the
+ *    residual back every iteration and therefore synchronise that stream.
+ *  - Complex arrays are interleaved (re, im): c128 = 2 x double, c64 = 2 x float.
+ *  - Block vectors are row-major (3*N_occ, L): row 3m+c is component c of
+ *    occupied dipole m, the L columns are orientations (reference layout,
+ *    bl_krylov/bl_krylov.py:27-55).  Full-cuboid vectors are (3*Nc, L) with
+ *    cells in C order (x slowest, z fastest), mvp_fft/mvp_fft.py:151-152.
+ *  - Return value: a BDDA_* status code.
+ *
+ * Reference interfaces replaced (block-DDA_Py v0.3.0, paths in that project):
+ *  mvp_fft/mvp_fft.py:13   build_interaction_tensor -> bdda_green_build (+ export)
+ *  mvp_fft/mvp_fft.py:97   fft_init                 -> bdda_green_build
+ *  mvp_fft/mvp_fft.py:122  fft_mvp                  -> bdda_fft_mvp
+ *  bl_krylov/bl_krylov.py:5   _build_scatter_index  -> bdda_occupancy_map
+ *  bl_krylov/bl_krylov.py:27  _block_mvp            -> bdda_block_mvp
+ *  bl_krylov/bl_krylov.py:58  bl_cocg_rq_jacobi_mvp_fft  -> bdda_cocg_rq
+ *  bl_krylov/bl_krylov.py:121 bl_bicgstab_jacobi_mvp_fft -> bdda_bicgstab
+ *  bl_dda/scatterer.py:135-161 set_interaction_matrix (diag_A, B) -> bdda_polarizability, bdda_incident_rhs
+ *  bl_dda/scatterer.py:182-227 E, C_abs, C_ext, S_fw, S_bk       -> bdda_observables
+ */
+#ifndef BDDA_H
+#define BDDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct bdda_plan bdda_plan;
+
+enum bdda_status {
+  BDDA_OK = 0,
+  BDDA_NOT_CONVERGED = 1, /* solver ran itermax iterations without err < tol (not an error
+                             in the reference, scatterer.py:175-176) */
+  BDDA_BREAKDOWN = 2,     /* singular or non-finite L x L system (numpy LinAlgError) */
+  BDDA_BAD_ARG = 3,       /* invalid size, pointer or option (reference ValueError) */
+  BDDA_NO_WORKSPACE = 4,  /* workspace pointer missing or plan tables not attached */
+  BDDA_TIMEOUT = 5,       /* a bounded device-side wait gave up */
+  BDDA_CUDA_ERROR = 6     /* a CUDA runtime call failed */
+};
+
+enum bdda_precision {
+  BDDA_C128 = 0, /* complex128 end to end */
+  BDDA_C64 = 1   /* complex64 storage, FP32 arithmetic */
+};
+
+const char* bdda_status_string(int status);
+int bdda_version(void);
+
+/* ---- plan: grid geometry and FFT factorisation (host object) -------------
+ * n = cuboid (Nx, Ny, Nz).  m = cyclic FFT grid; NULL chooses, per axis, the
+ * smallest even 7-smooth length >= 2N (= 2N, the reference's doubled grid,
+ * whenever 2N is 7-smooth).  Any m >= 2N-1 gives the same product, because
+ * only displacements |d| <= N-1 reach the cropped output.
+ * replaces the implicit grid of mvp_fft/mvp_fft.py:43-45,155 */
+int bdda_plan_create(const int n[3], const int m[3], bdda_plan** out);
+void bdda_plan_destroy(bdda_plan* plan);
+int bdda_plan_grid(const bdda_plan* plan, int m[3]);
+int bdda_plan_radices(const bdda_plan* plan, int axis, int radices[12], int* nstage);
+/* Twiddle and digit-reversal tables: the caller gives a device buffer of
+ * bdda_plan_table_bytes(); the plan uploads into it and keeps the pointer. */
+size_t bdda_plan_table_bytes(const bdda_plan* plan);
+int bdda_plan_attach_tables(bdda_plan* plan, void* dev_tables, void* stream);
+
+/* ---- Green's tensor spectrum ----------------------------------------------
+ * A'(r) (mvp_fft/mvp_fft.py:77-84) on the cyclic grid, 6 unique components
+ * (xx, xy, xz, yy, yz, zz), forward FFT over the three axes.  Stored in the
+ * library's own order (x-pencil major, spectra digit-reversed).
+ * replaces mvp_fft/mvp_fft.py:13 build_interaction_tensor + :97 fft_init */
+size_t bdda_green_bytes(const bdda_plan* plan, int prec);
+size_t bdda_green_build_workspace_bytes(const bdda_plan* plan);
+int bdda_green_build(const bdda_plan* plan, double lf, double k, void* ghat_c128, void* work,
+                     void* stream);
+/* Real-space tensor A'(r) in natural order (Mx, My, Mz, 3, 3) c128, origin and
+ * non-physical displacements zero: the reference's array when m = 2n.
+ * replaces mvp_fft/mvp_fft.py:13 build_interaction_tensor */
+int bdda_green_real(const bdda_plan* plan, double lf, double k, void* full_c128, void* stream);
+/* c128 -> c64 rounding copy for the FP32 product */
+int bdda_green_convert(const bdda_plan* plan, const void* ghat_c128, void* ghat_c64, void* stream);
+/* Library order <-> natural (Mx, My, Mz, 3, 3) c128 (the reference's Au_til
+ * layout when m = 2n).  Import reads the upper triangle. */
+int bdda_green_export(const bdda_plan* plan, const void* ghat_c128, void* full_c128, void* stream);
+int bdda_green_import(const bdda_plan* plan, const void* full_c128, void* ghat_c128, void* stream);
+
+/* ---- matrix-vector products ------------------------------------------------ */
+size_t bdda_mvp_workspace_bytes(const bdda_plan* plan, int prec, int L);
+/* cell_map[cell] = m for address[m] = cell, -1 elsewhere (Nc int32).
+ * replaces bl_krylov/bl_krylov.py:5 _build_scatter_index */
+int bdda_occupancy_map(const bdda_plan* plan, const int64_t* address, int n_occ,
+                       int32_t* cell_map, void* stream);
+/* Y_full = A_off P_full on the full cuboid, (3 Nc, L).
+ * replaces mvp_fft/mvp_fft.py:122 fft_mvp */
+int bdda_fft_mvp(const bdda_plan* plan, int prec, int L, const void* ghat, const void* P_full,
+                 void* Y_full, void* work, void* stream);
+/* out = jpre * (diag * S + gather(A_off scatter(S))), S and out (3 N_occ, L).
+ * replaces bl_krylov/bl_krylov.py:27 _block_mvp */
+int bdda_block_mvp(const bdda_plan* plan, int prec, int L, const void* ghat,
+                   const int32_t* cell_map, const void* diag, const void* jpre, const void* S,
+                   void* out, void* work, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BDDA_H */

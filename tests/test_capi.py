@@ -1,0 +1,85 @@
+"""libbdda.so loads, exports every entry point of include/bdda.h, and its
+host-only plan logic behaves (no GPU needed)."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+from bdda_b200 import _lib
+
+HEADER = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include", "bdda.h")
+
+
+def header_functions():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(bdda_\w+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = _lib.load()
+    names = header_functions()
+    assert len(names) >= 15
+    for name in names:
+        assert hasattr(lib, name), name
+
+
+def test_bindings_cover_the_header_exactly():
+    assert sorted(_lib.PROTOTYPES) == header_functions()
+
+
+def test_status_strings():
+    assert _lib.status_string(_lib.OK) == "ok"
+    assert "singular" in _lib.status_string(_lib.BREAKDOWN)
+    with pytest.raises(ValueError):
+        _lib.check(_lib.BAD_ARG, "x")
+    with pytest.raises(np.linalg.LinAlgError):
+        _lib.check(_lib.BREAKDOWN, "x")
+    assert _lib.check(_lib.NOT_CONVERGED, "x") == _lib.NOT_CONVERGED
+
+
+def _plan(n, m=None):
+    lib = _lib.load()
+    h = C.c_void_p()
+    st = lib.bdda_plan_create(_lib.int3(n), None if m is None else _lib.int3(m), C.byref(h))
+    if st != _lib.OK:
+        return st, None, None
+    mm = (C.c_int * 3)()
+    lib.bdda_plan_grid(h, mm)
+    rad = []
+    for a in range(3):
+        r = (C.c_int * 12)()
+        ns = C.c_int()
+        lib.bdda_plan_radices(h, a, r, C.byref(ns))
+        rad.append([r[i] for i in range(ns.value)])
+    lib.bdda_plan_destroy(h)
+    return st, list(mm), rad
+
+
+def smooth7(m):
+    for p in (2, 3, 5, 7):
+        while m % p == 0:
+            m //= p
+    return m == 1
+
+
+@pytest.mark.parametrize("n", [(28, 28, 28), (17, 17, 17), (93, 112, 174), (5, 6, 7), (1, 1, 1), (11, 13, 37)])
+def test_plan_grid_choice(n):
+    st, m, rad = _plan(n)
+    assert st == _lib.OK
+    for N, M, r in zip(n, m, rad):
+        assert M >= 2 * N and M % 2 == 0 and smooth7(M)
+        if smooth7(2 * N):
+            assert M == 2 * N          # the reference's doubled grid
+        assert int(np.prod(r)) == M and set(r) <= {2, 3, 4, 5, 7, 8}
+        # nothing smaller qualifies
+        assert not any(smooth7(x) for x in range(2 * N, M, 2))
+
+
+def test_plan_accepts_explicit_grid_and_rejects_short_or_rough():
+    assert _plan((5, 4, 6), (9, 10, 15))[0] == _lib.OK
+    assert _plan((5, 4, 6), (8, 10, 15))[0] == _lib.BAD_ARG     # 8 < 2*5-1
+    assert _plan((5, 4, 6), (11, 10, 15))[0] == _lib.BAD_ARG    # 11 is not 7-smooth
+    assert _plan((0, 4, 6))[0] == _lib.BAD_ARG
