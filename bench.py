@@ -1,0 +1,360 @@
+#!/usr/bin/env python
+"""Orientations/s to relative residual 1e-5 on one GRE particle, block-BiCGSTAB.
+
+Workload (the mixed-precision single-particle configuration): Gaussian
+random ellipsoid with size parameter x = 20 (wl_0 = 1, m_m = 1.33), ab 0.7,
+bc 0.8, beta 0.1, surface seed 1, spacing lambda_m/16 -> 93 x 112 x 174
+lattice with 438,606 dipoles (geometry produced by the reference's shape
+model and shipped in tests/golden/geometry_cfg2.npz), birefringent m_p =
+(1.55+0.001i, 1.60+0.001i, 1.52+0.002i), L = 64 SO(3)-uniform orientations
+(seed 2).  One step = polarizability + right-hand side + block solve to
+||R||/||M^-1 B|| < 1e-5 + observables, for all 64 orientations.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl bdda|reference] [--form fp64]
+
+Prints one JSON line on rank 0.  Multi-GPU runs are replicas (each rank
+solves its own copy; there is no data exchange on this path).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(REPO, "block-dda_py_b200"))
+sys.path.insert(0, REPO)
+
+GEOMETRY = os.path.join(REPO, "tests", "golden", "geometry_cfg2.npz")
+METRIC = "orientations/s to rel-res 1e-5: plain FP64 vs FP32+refine+NN warm start, 1 B200"
+TOL = 1e-5
+ITERMAX = 500
+# Block-BiCGSTAB iterations to 1e-5 for an 8-orientation chunk of this
+# workload (orientations 0-7), as run by the FP64 GPU path (iter_fin = 20).
+# The CPU reference runs the same algorithm (iteration counts agree within 1),
+# so its throughput is extrapolated from a timed sample of iterations.
+REF_ITERS_PER_CHUNK = 21
+
+
+def workload_config(L):
+    return {"workload": "GRE x=20 ab0.7 bc0.8 beta0.1 seed1, m_m 1.33, lambda_m/16 -> 93x112x174 lattice, "
+                        "438606 dipoles, L=%d SO(3) orientations (seed 2), block-BiCGSTAB to 1e-5" % L,
+            "lattice": [93, 112, 174], "n_dipoles": 438606, "orientations": L, "solver": "block-BiCGSTAB",
+            "tol": TOL, "l2": "inputs larger than L2 (working set ~35 GB >> 126 MB)"}
+
+
+def load_workload(L):
+    from bdda_b200.inputs import load_geometry
+    geo = load_geometry(GEOMETRY)
+    return geo, geo["euler"][:L]
+
+
+# ---------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200", "-f", self.path],
+                                         stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return None
+        rows = []
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ---------------------------------------------------------------------------
+# algorithmic bytes of one block MVP (five pencil passes)
+# ---------------------------------------------------------------------------
+def mvp_pass_bytes(n, m, n_occ, L, s):
+    """Bytes each pass must move at minimum: every value it reads or writes once."""
+    Nx, Ny, Nz = n
+    Mx, My, Mz = m
+    C = 3 * L
+    nc = Nx * Ny * Nz
+    zrows, yrows = Nx * Ny * Mz, Nx * My * Mz
+    return [n_occ * C * s + nc * 4 + zrows * C * s,              # Z: gather S, forward z
+            zrows * C * s + yrows * C * s,                       # Y: Ny rows in, My out
+            2 * yrows * C * s + Mx * My * Mz * 6 * s,            # X: in place + Green spectrum
+            yrows * C * s + zrows * C * s,                       # Y^-1
+            zrows * C * s + 2 * n_occ * C * s + 2 * 3 * n_occ * s + nc * 4]   # Z^-1 + epilogue
+
+
+# ---------------------------------------------------------------------------
+# the GPU arm
+# ---------------------------------------------------------------------------
+def run_bdda(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+    from bdda_b200 import _lib
+    from bl_dda import scatterer as sc
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    sc.DiscreteDipoles.verbose = False
+    lib = _lib.load()
+    L = args.L
+    geo, euler = load_workload(L)
+
+    def make_dd():
+        t = sc.Target("gre", geo["lattice_n"], geo["lattice_lf"], geo["grid"], geo["is_in"], geo["m_p_xyz"])
+        dd = sc.DiscreteDipoles(t, sc.IncidentField(float(geo["wl_0"]), float(geo["m_m"]), euler))
+        dd.tol, dd.itermax = TOL, ITERMAX
+        dd.precision = None if args.form == "fp64" else args.form
+        return dd
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- set-up (untimed): resident geometry and Green's spectrum ----
+    dd = make_dd()
+    t0 = time.perf_counter()
+    dd.set_interaction_matrix()
+    torch.cuda.synchronize()
+    green_s = time.perf_counter() - t0
+    green = dd.Au_til
+
+    def device_step():
+        dd.set_interaction_matrix(green=green)
+        dd.solve_matrix_equation()
+        return dd.observables()
+
+    for _ in range(args.warmup):
+        device_step()
+    iters = dd.iter_fin + 1
+    converged = dd.converge
+    n0 = lib.bdda_launch_count()
+    lib.bdda_profile_enable(1)
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local_rank) as clk:
+        e0.record()
+        for _ in range(args.steps):
+            device_step()
+        e1.record()
+        barrier()
+    ms = max_over_ranks(e0.elapsed_time(e1) / args.steps)
+    launches = (lib.bdda_launch_count() - n0) / args.steps
+    pass_ms = (_lib.C.c_double * 5)()
+    nmvp = _lib.C.c_longlong(0)
+    lib.bdda_profile_read(pass_ms, _lib.C.byref(nmvp))
+    lib.bdda_profile_enable(0)
+    clocks = clk.summary()
+
+    # ---- end to end through the public API, host numpy in and out ----
+    def e2e_step():
+        d = make_dd()
+        d.set_interaction_matrix()
+        d.solve_matrix_equation()
+        res = (d.compute_C_abs(), d.compute_C_ext(), d.compute_PCAS_observable_S_fw(),
+               d.compute_OCBS_observable_S_bk())
+        return d, res
+
+    d_e2e, _ = e2e_step()      # warm
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(max(1, args.steps)):
+        d_e2e, _ = e2e_step()
+    torch.cuda.synchronize()
+    e2e_s = max_over_ranks((time.perf_counter() - t0) / max(1, args.steps))
+    h2d = sum(d_e2e._dev[k].numel() * d_e2e._dev[k].element_size() for k in ("pos", "vec", "e0", "u_inc"))
+    h2d += d_e2e._dev["occ"].address_dev.numel() * 8
+    d2h = L * 12 * 8
+
+    # ---- roofline of the product (measured above over the timed region) ----
+    plan = green.plan
+    s = 16 if args.form == "fp64" else 8
+    pb = mvp_pass_bytes(plan.n, plan.m, dd.num_element_occupy, L, s)
+    peaks = {}
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except (OSError, ValueError):
+        pass
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    n_mvp = max(1, nmvp.value)
+    per_pass_ms = [pass_ms[i] / n_mvp for i in range(5)]
+    mvp_ms = sum(per_pass_ms)
+    achieved = sum(pb) / (mvp_ms * 1e-3) / 1e9
+    passes = [{"pass": nm, "ms": round(t, 3), "GB/s": round(b / (t * 1e-3) / 1e9, 1),
+               "frac": round(b / (t * 1e-3) / 1e9 / peak, 3)}
+              for nm, t, b in zip(["Z", "Y", "X", "Y^-1", "Z^-1"], per_pass_ms, pb)]
+
+    result = {
+        "metric": METRIC,
+        "value": round(world * L / (ms * 1e-3), 3),
+        "unit": "orientations/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(ms, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "complex128" if args.form == "fp64" else "complex64+complex128",
+        "form": args.form,
+        "data": "synthetic: reference GRE geometry (seed 1) and SO(3) orientations (seed 2)",
+        "config": dict(workload_config(L), parallelism="replicas x%d" % world,
+                       green_build_s=round(green_s, 4), iterations=iters, converged=converged),
+        "e2e": {"value": round(world * L / e2e_s, 3), "unit": "orientations/s",
+                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                "includes": "Target/IncidentField/DiscreteDipoles from host arrays, Green build, solve, "
+                            "observables to host"},
+        "gpu_launches": int(round(launches)),
+        "clocks": clocks,
+        "roofline": {"kernel": "block MVP (5 pencil passes)", "bound": "hbm",
+                     "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 3), "traffic": None, "peak_source": peak_src,
+                     "alg_bytes_per_mvp": int(sum(pb)), "mvp_ms": round(mvp_ms, 3), "mvps_timed": n_mvp,
+                     "passes": passes},
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        result["cpu_baseline"] = cpu_reference(geo, L, sample_iters=1)
+    return result
+
+
+# ---------------------------------------------------------------------------
+# the CPU reference (the oracle's restatement of the reference algorithm)
+# ---------------------------------------------------------------------------
+def cpu_reference(geo, L_total, sample_iters=1, chunk=8, threads=None):
+    """Reference throughput from a bounded sample: one L=8 chunk, timed pieces.
+
+    T(64) = fft_init + (64/8) x [RHS + REF_ITERS_PER_CHUNK x t_iter + observables]
+    """
+    from oracle import dda_oracle as O
+    threads = threads or os.cpu_count() or 1
+    O.FFT_WORKERS = threads
+    n = geo["lattice_n"]
+    lf = geo["lattice_lf"]
+    address = geo["address"]
+    pos = geo["grid"][address]
+    euler = geo["euler"][:chunk]
+    g = O.incident_geometry(float(geo["wl_0"]), float(geo["m_m"]), euler)
+    t0 = time.perf_counter()
+    Ghat = O.fft_init(n, 3, lf, g["k"])
+    t_green = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    eper_r, _, diag = O.polarizability(geo["m_p_xyz"], float(geo["m_m"]), lf, g["k"], address.size)
+    B = O.rhs(g["k"], g["u_inc"], g["e0_inc"], pos)
+    t_rhs = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    X, _, _ = O.bicgstab(n, 3, address, Ghat, diag, B, TOL, sample_iters)
+    t_iter = (time.perf_counter() - t0) / sample_iters
+    t0 = time.perf_counter()
+    O.observables(X, g, pos, eper_r, lf)
+    t_obs = time.perf_counter() - t0
+    chunks = L_total / chunk
+    total = t_green + chunks * (t_rhs + REF_ITERS_PER_CHUNK * t_iter + t_obs)
+    return {"value": round(L_total / total, 5), "unit": "orientations/s", "cores": threads, "kind": "port",
+            "sample": "oracle (scipy.fft/numpy restatement of the reference) on one 8-orientation chunk: "
+                      "fft_init %.1fs, RHS %.2fs, %d BiCGSTAB iteration(s) %.1fs each, observables %.2fs; "
+                      "extrapolated to %d iterations x %d chunks (DDA_FFT_WORKERS=%d)"
+                      % (t_green, t_rhs, sample_iters, t_iter, t_obs, REF_ITERS_PER_CHUNK, chunks, threads)}
+
+
+def run_reference(args, rank, world):
+    geo, _ = load_workload(args.L)
+    steps = []
+    for i in range(args.warmup + args.steps):
+        cb = cpu_reference(geo, args.L, sample_iters=1)
+        if i >= args.warmup:
+            steps.append(cb)
+    vals = [s["value"] for s in steps]
+    v = statistics.median(vals)
+    cb = dict(steps[-1], value=v)
+    return {"metric": METRIC, "value": v, "unit": "orientations/s", "impl": "reference", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * args.L / v, 1),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "complex128",
+            "data": "synthetic: reference GRE geometry (seed 1) and SO(3) orientations (seed 2)",
+            "config": dict(workload_config(args.L), parallelism="cpu"),
+            "cpu_baseline": cb,
+            "e2e": {"value": v, "unit": "orientations/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="bdda", choices=["bdda", "reference"])
+    ap.add_argument("--form", default="fp64", choices=["fp64"])
+    ap.add_argument("--L", type=int, default=64)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        print(json.dumps(run_reference(args, rank, world)), flush=True)
+        return
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    try:
+        res = run_bdda(args, rank, world, local_rank)
+        if rank == 0:
+            print(json.dumps(res), flush=True)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

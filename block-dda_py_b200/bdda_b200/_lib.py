@@ -18,6 +18,8 @@ LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libbdda.so"
 OK, NOT_CONVERGED, BREAKDOWN, BAD_ARG, NO_WORKSPACE, TIMEOUT, CUDA_ERROR = range(7)
 # precisions (include/bdda.h: enum bdda_precision)
 C128, C64 = 0, 1
+# solvers (include/bdda.h: enum bdda_solver_kind)
+BICGSTAB, COCG_RQ = 0, 1
 
 _vp = C.c_void_p
 _sz = C.c_size_t
@@ -47,6 +49,20 @@ PROTOTYPES = {
     "bdda_occupancy_map": (_i, [_vp, _vp, _i, _vp, _vp]),
     "bdda_fft_mvp": (_i, [_vp, _i, _i, _vp, _vp, _vp, _vp, _vp]),
     "bdda_block_mvp": (_i, [_vp, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "bdda_solver_workspace_bytes": (_sz, [_vp, _i, _i, _i, _i]),
+    "bdda_polarizability": (_i, [_i, C.POINTER(_d), _d, _d, _d, _vp, _vp, _vp]),
+    "bdda_incident_rhs": (_i, [_i, _i, _d, _vp, _vp, _vp, _vp, _vp]),
+    "bdda_observables_workspace_bytes": (_sz, [_i]),
+    "bdda_launch_count": (C.c_ulonglong, []),
+    "bdda_profile_enable": (_i, [_i]),
+    "bdda_profile_read": (_i, [C.POINTER(_d), C.POINTER(C.c_longlong)]),
+    "bdda_observables": (_i, [_i, _i, _d, _d, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "bdda_solve": (_i, [_vp, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _vp, _d, _i, _vp, _pi,
+                        C.POINTER(_d), C.POINTER(_d), _vp, _sz, _vp]),
+    "bdda_bicgstab": (_i, [_vp, _i, _i, _i, _vp, _vp, _vp, _vp, _vp, _d, _i, _vp, _pi,
+                           C.POINTER(_d), C.POINTER(_d), _vp, _sz, _vp]),
+    "bdda_cocg_rq": (_i, [_vp, _i, _i, _i, _vp, _vp, _vp, _vp, _vp, _d, _i, _vp, _pi,
+                          C.POINTER(_d), C.POINTER(_d), _vp, _sz, _vp]),
 }
 
 

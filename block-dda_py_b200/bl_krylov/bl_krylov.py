@@ -7,6 +7,8 @@ small L x L solves and the block updates all run in libbdda.so.
 """
 from __future__ import annotations
 
+import ctypes as C
+
 import numpy as np
 import torch
 
@@ -54,3 +56,76 @@ def _block_mvp(n, f, Au_til, full_idx, DIAG_A, S, jpre, precision=None):
                                           ptr(d), ptr(j), ptr(Sd), ptr(out), ptr(work),
                                           stream_ptr(plan.device)), "bdda_block_mvp")
     return out.cpu().numpy() if to_numpy else out
+
+
+def _solve(kind, n, f, address, Au_til, DIAG_A, B, tol, itermax, X0=None, precision=None,
+           history=None, verbose=False):
+    """Shared body of the two block solvers (C entry point ``bdda_solve``)."""
+    if f != 3:
+        raise ValueError("only f=3 (electric dipoles) is supported.")
+    g = as_green(n, Au_til)
+    plan = g.plan
+    prec = precision_code(precision)
+    occ = address if isinstance(address, Occupancy) else Occupancy(plan, address)
+    to_numpy = not isinstance(B, torch.Tensor)
+    Bd = to_device(B, torch.complex128, plan.device)
+    if Bd.dim() != 2 or Bd.shape[0] != 3 * occ.n_occ:
+        raise ValueError("B must be (%d, L), got %r" % (3 * occ.n_occ, tuple(Bd.shape)))
+    L = int(Bd.shape[1])
+    if L > 64:
+        raise ValueError("at most 64 right-hand sides per block solve (got L=%d); split the block" % L)
+    diag = to_device(DIAG_A, torch.complex128, plan.device).reshape(-1)
+    if diag.numel() != 3 * occ.n_occ:
+        raise ValueError("DIAG_A must have %d entries" % (3 * occ.n_occ))
+    X0d = None if X0 is None else to_device(X0, torch.complex128, plan.device).reshape(Bd.shape).contiguous()
+    lib = _lib.load()
+    X = torch.empty_like(Bd)
+    nbytes = int(lib.bdda_solver_workspace_bytes(plan.handle, kind, prec, L, occ.n_occ))
+    work = torch.empty(max(nbytes, 16), dtype=torch.uint8, device=plan.device)
+    itermax = int(itermax)
+    hist = (C.c_double * max(itermax, 1))()
+    it = C.c_int(0)
+    err = C.c_double(float("inf"))
+    status = lib.bdda_solve(plan.handle, kind, prec, L, occ.n_occ, ptr(g.ghat(prec)), ptr(occ.cell_map),
+                            ptr(diag), ptr(Bd), ptr(X0d), float(tol), itermax, ptr(X), C.byref(it),
+                            C.byref(err), hist, ptr(work), nbytes, stream_ptr(plan.device))
+    _lib.check(status, "bdda_solve")
+    ran = 0 if itermax == 0 else it.value + 1
+    if history is not None:
+        history.extend(hist[i] for i in range(ran))
+    if verbose:
+        for i in range(ran):
+            print("iter= {:}, err= {:.4f}".format(i, hist[i]))
+    del work
+    return (X.cpu().numpy() if to_numpy else X), it.value, err.value
+
+
+def bl_cocg_rq_jacobi_mvp_fft(n, f, address, Au_til, DIAG_A, B, tol, itermax, X0=None,
+                              precision=None, history=None, verbose=False):
+    """Block-COCG-rq with Jacobi preconditioning (bl_krylov.py:58-118).
+
+    Returns ``(X, iter_fin, err_fin)`` with the reference's meaning: X the
+    (f*N_occ, L) solution, iter_fin the 0-based index of the last iteration,
+    err_fin = ||xi||_F / ||M^-1 B||_F at that iteration.  Not converging is
+    not an error.  Extra keywords (all optional): ``X0`` initial guess,
+    ``precision`` "c128" (default) or "c64", ``history`` list receiving the
+    per-iteration residuals, ``verbose`` prints them like the reference.
+    The QR factorisations are CholeskyQR (R with real positive diagonal
+    instead of LAPACK's Householder signs); X and err are independent of
+    that choice.
+    """
+    return _solve(_lib.COCG_RQ, n, f, address, Au_til, DIAG_A, B, tol, itermax, X0, precision,
+                  history, verbose)
+
+
+def bl_bicgstab_jacobi_mvp_fft(n, f, address, Au_til, DIAG_A, B, tol, itermax, X0=None,
+                               precision=None, history=None, verbose=False):
+    """Block-BiCGSTAB with Jacobi preconditioning (bl_krylov.py:121-187).
+
+    Returns ``(X, iter_fin, err_fin)`` as the reference; err_fin is the
+    recursively updated ||R||_F / ||M^-1 B||_F.  A singular R0^H V raises
+    numpy.linalg.LinAlgError like numpy.linalg.solve.  Extra keywords as for
+    :func:`bl_cocg_rq_jacobi_mvp_fft`.
+    """
+    return _solve(_lib.BICGSTAB, n, f, address, Au_til, DIAG_A, B, tol, itermax, X0, precision,
+                  history, verbose)

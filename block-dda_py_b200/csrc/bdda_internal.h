@@ -22,6 +22,12 @@ struct bdda_plan {
 
 namespace bdda {
 
+// Kernel launches issued by the library (all threads, all devices).
+void count_launch(int n = 1);
+// Optional per-pass timing of every block MVP (events on the launching stream).
+bool profiling();
+void profile_mark(int pass, cudaStream_t st);   // pass 0..5: before Z, after Z, Y, X, Y^-1, Z^-1
+
 #define BDDA_CUDA_TRY(expr)                      \
   do {                                           \
     cudaError_t e_ = (expr);                     \

@@ -218,6 +218,7 @@ static int launch_lt(PassArgs a, int64_t P0, cudaStream_t st) {
   BDDA_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   kern<<<(unsigned)nblk, 256, smem, st>>>(a);
   BDDA_CUDA_TRY(cudaGetLastError());
+  count_launch();
   return BDDA_OK;
 }
 
@@ -253,6 +254,8 @@ static int run_mvp(const bdda_plan* plan, int L, const T* ghat, const int32_t* c
   memset(&b, 0, sizeof(b));
   b.L = L;
   b.C = C;
+  const bool prof = profiling();
+  if (prof) profile_mark(0, st);
 
   {  // Z: gather + forward z
     PassArgs a = b;
@@ -262,6 +265,7 @@ static int run_mvp(const bdda_plan* plan, int L, const T* ghat, const int32_t* c
     a.S = src; a.src = src;
     a.dst = F; a.dst_p0 = My * Mz * C; a.dst_p1 = Mz * C; a.dst_row = C;
     BDDA_TRY((launch_pass<T, K_FWD_GATHER>(a, Nx, pick_lt((int)Mz, L, sizeof(T)), st)));
+    if (prof) profile_mark(1, st);
   }
   PassArgs ay = b;  // Y and Y^-1 share the pencil geometry
   ay.ax = plan->ax[1]; ay.tw = table_ptr<T>(plan, TwOff<T>::get(plan, 1));
@@ -272,6 +276,7 @@ static int run_mvp(const bdda_plan* plan, int L, const T* ghat, const int32_t* c
     PassArgs a = ay;
     a.n_in = (int)Ny; a.n_out = (int)My;
     BDDA_TRY((launch_pass<T, K_FWD>(a, Nx, lty, st)));
+    if (prof) profile_mark(2, st);
   }
   {  // X: forward, Green multiply, inverse
     PassArgs a = b;
@@ -281,11 +286,13 @@ static int run_mvp(const bdda_plan* plan, int L, const T* ghat, const int32_t* c
     a.src_p0 = a.dst_p0 = Mz * C; a.src_p1 = a.dst_p1 = C; a.src_row = a.dst_row = My * Mz * C;
     a.ghat = ghat;
     BDDA_TRY((launch_pass<T, K_CONV>(a, My, pick_lt((int)Mx, L, sizeof(T)), st)));
+    if (prof) profile_mark(3, st);
   }
   {
     PassArgs a = ay;
     a.n_in = (int)My; a.n_out = (int)Ny;
     BDDA_TRY((launch_pass<T, K_INV>(a, Nx, lty, st)));
+    if (prof) profile_mark(4, st);
   }
   {  // Z^-1 + crop + epilogue
     PassArgs a = b;
@@ -296,6 +303,7 @@ static int run_mvp(const bdda_plan* plan, int L, const T* ghat, const int32_t* c
     a.S = src; a.diag = diag; a.jpre = jpre; a.dst = out;
     a.scale = 1.0 / (double)(Mx * My * Mz);
     BDDA_TRY((launch_pass<T, K_INV_SCATTER>(a, Nx, pick_lt((int)Mz, L, sizeof(T)), st)));
+    if (prof) profile_mark(5, st);
   }
   return BDDA_OK;
 }
@@ -560,6 +568,7 @@ int bdda_green_real(const bdda_plan* p, double lf, double k, void* full, void* s
   a.k = k;
   green_real_kernel<<<148 * 8, 256, 0, (cudaStream_t)stream>>>(a, static_cast<double2*>(full));
   BDDA_CUDA_TRY(cudaGetLastError());
+  count_launch();
   return BDDA_OK;
 }
 
@@ -569,6 +578,7 @@ int bdda_green_convert(const bdda_plan* p, const void* g64, void* g32, void* str
   convert_kernel<<<148 * 8, 256, 0, (cudaStream_t)stream>>>(static_cast<const double2*>(g64),
                                                             static_cast<float2*>(g32), n);
   BDDA_CUDA_TRY(cudaGetLastError());
+  count_launch();
   return BDDA_OK;
 }
 
@@ -587,6 +597,7 @@ static int green_reorder(const bdda_plan* p, const void* in, void* out, void* st
     green_reorder_kernel<false><<<148 * 8, 256, 0, (cudaStream_t)stream>>>(
         g, static_cast<const double2*>(in), static_cast<double2*>(out));
   BDDA_CUDA_TRY(cudaGetLastError());
+  count_launch();
   return BDDA_OK;
 }
 
@@ -612,6 +623,7 @@ int bdda_occupancy_map(const bdda_plan* p, const int64_t* address, int n_occ, in
   if (n_occ > 0) {
     occupancy_kernel<<<(n_occ + 255) / 256, 256, 0, st>>>(address, n_occ, nc, cell_map);
     BDDA_CUDA_TRY(cudaGetLastError());
+    count_launch();
   }
   return BDDA_OK;
 }

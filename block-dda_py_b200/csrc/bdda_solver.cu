@@ -1,0 +1,623 @@
+// Block Krylov solvers on the device: block-BiCGSTAB and block-COCG-rq with
+// Jacobi (diagonal) left preconditioning, built on the fused block MVP.
+//
+// The host loop launches kernels only; every coefficient (alpha, beta, zeta,
+// xi, tau) lives in device memory.  Once per iteration a 16-byte status
+// (relative residual, breakdown flag) is read back to decide termination,
+// exactly where the reference tests ``err < tol`` (bl_krylov.py:110,181).
+#include <cmath>
+#include <cstring>
+#include <type_traits>
+#include <utility>
+
+#include "bdda_blas.cuh"
+#include "bdda_internal.h"
+#include "bdda_small.cuh"
+
+namespace bdda {
+
+struct SolverState {
+  double2 zeta, negzeta;
+  double red[4];
+  double bnorm;
+  double err;
+  int bad;      // 1: zero pivot (singular small system), 2: non-finite values
+  int pad;
+};
+
+struct Layout {
+  size_t field, vec[8], diag, jpre, partial, small, state, total;
+};
+
+constexpr int kVecs = 8;
+constexpr int kSmallMats = 16;
+
+static size_t al(size_t x) { return (x + 255) & ~(size_t)255; }
+
+static Layout layout(const bdda_plan* p, int prec, int L, int n_occ) {
+  Layout o;
+  const size_t cb = cplx_bytes(prec);
+  const size_t vbytes = (size_t)3 * n_occ * L * cb;
+  size_t off = 0;
+  o.field = off; off = al(off + bdda_mvp_workspace_bytes(p, prec, L));
+  for (int v = 0; v < kVecs; ++v) { o.vec[v] = off; off = al(off + vbytes); }
+  o.diag = off; off = al(off + (size_t)3 * n_occ * cb);
+  o.jpre = off; off = al(off + (size_t)3 * n_occ * cb);
+  o.partial = off; off = al(off + (size_t)kRedBlocks * 2 * kMaxL * kMaxL * sizeof(double2));
+  o.small = off; off = al(off + (size_t)kSmallMats * kMaxL * kMaxL * sizeof(double2) + 64 * sizeof(int));
+  o.state = off; off = al(off + sizeof(SolverState));
+  o.total = off;
+  return o;
+}
+
+// ---- elementwise set-up kernels -------------------------------------------------
+// jpre = 1/diag and Bj = B * jpre in complex128 (bl_krylov.py:84-87,146-149),
+// then stored in the working precision
+template <typename T>
+__global__ void prepare_kernel(const double2* diag, const double2* B, int64_t nrow, int L, T* diagT,
+                               T* jpreT, T* Bj) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nrow * L;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = i / L;
+    const double2 d = diag[r];
+    const double2 j = zdiv(make_double2(1.0, 0.0), d);
+    Bj[i] = from_d2<T>(zmul(B[i], j));
+    if (i % L == 0) {
+      diagT[r] = from_d2<T>(d);
+      jpreT[r] = from_d2<T>(j);
+    }
+  }
+}
+
+template <typename T>
+__global__ void convert_in_kernel(const double2* in, T* out, int64_t n) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = from_d2<T>(in[i]);
+}
+
+template <typename T>
+__global__ void convert_out_kernel(const T* in, double2* out, int64_t n) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = to_d2(in[i]);
+}
+
+// ---- one-CTA step kernels -------------------------------------------------------
+struct SmallPtrs {
+  double2 *g2, *lu, *alpha, *negalpha, *beta, *tmp, *xi, *tau, *qq, *rinv, *alphaxi, *r;
+  int* piv;
+};
+
+static SmallPtrs small_ptrs(unsigned char* base) {
+  double2* m = reinterpret_cast<double2*>(base);
+  const size_t S = (size_t)kMaxL * kMaxL;
+  SmallPtrs s;
+  s.g2 = m;            // two matrices
+  s.lu = m + 2 * S;
+  s.alpha = m + 3 * S;
+  s.negalpha = m + 4 * S;
+  s.beta = m + 5 * S;
+  s.tmp = m + 6 * S;   // two matrices
+  s.xi = m + 8 * S;
+  s.tau = m + 9 * S;
+  s.qq = m + 10 * S;
+  s.rinv = m + 11 * S;
+  s.alphaxi = m + 12 * S;
+  s.r = m + 13 * S;
+  s.piv = reinterpret_cast<int*>(m + kSmallMats * S);
+  return s;
+}
+
+__device__ __forceinline__ void flag_nonfinite(const double2* a, int n, SolverState* st) {
+  for (int e = threadIdx.x; e < n; e += blockDim.x)
+    if (!zfinite(a[e])) atomicCAS(&st->bad, 0, 2);
+  __syncthreads();
+}
+
+// ||.|| from a sum of squares; optionally the initial residual norm
+__global__ void norm_kernel(const double* partial, int nblk, SolverState* st, int set_bnorm) {
+  double s = 0.0;
+  for (int b = threadIdx.x; b < nblk; b += blockDim.x) s += partial[b];
+  __shared__ double red[32];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+    const double nrm = sqrt(t);
+    if (set_bnorm) st->bnorm = nrm;
+    st->err = nrm / st->bnorm;
+    if (!isfinite(st->err)) atomicCAS(&st->bad, 0, 2);
+  }
+}
+
+// BiCGSTAB: LU(RV), alpha = RV^-1 (R0^H R)   (bl_krylov.py:166-167)
+__global__ void bicg_alpha_kernel(SmallPtrs s, int L, SolverState* st) {
+  extern __shared__ double2 sm[];
+  double2* a = sm;
+  double2* b = sm + L * L;
+  __shared__ int piv[kMaxL];
+  __shared__ int bad;
+  if (threadIdx.x == 0) bad = 0;
+  block_copy(a, s.g2, L * L);
+  block_copy(b, s.g2 + L * L, L * L);
+  __syncthreads();
+  lu_factor(a, L, piv, &bad);
+  if (!bad) lu_solve(a, piv, L, b, L);
+  for (int e = threadIdx.x; e < L * L; e += blockDim.x) {
+    s.lu[e] = a[e];
+    s.alpha[e] = b[e];
+    s.negalpha[e] = make_double2(-b[e].x, -b[e].y);
+  }
+  for (int e = threadIdx.x; e < L; e += blockDim.x) s.piv[e] = piv[e];
+  __syncthreads();
+  if (threadIdx.x == 0 && bad == 1) atomicExch(&st->bad, 1);
+  if (threadIdx.x == 0 && bad == 2) atomicCAS(&st->bad, 0, 2);
+  flag_nonfinite(b, L * L, st);
+}
+
+// BiCGSTAB: zeta = tr(Z^H T) / tr(Z^H Z); beta = RV^-1 (-R0^H Z)   (bl_krylov.py:173,184)
+__global__ void bicg_zeta_beta_kernel(SmallPtrs s, int L, const double* dot_partial, int nblk,
+                                      SolverState* st) {
+  extern __shared__ double2 sm[];
+  double2* a = sm;
+  double2* b = sm + L * L;
+  __shared__ int piv[kMaxL];
+  __shared__ double tot[3];
+  __shared__ int singular;
+  if (threadIdx.x == 0) singular = (st->bad == 1);
+  if (threadIdx.x < 3) {
+    double acc = 0.0;
+    for (int k = 0; k < nblk; ++k) acc += dot_partial[k * 3 + threadIdx.x];
+    tot[threadIdx.x] = acc;
+  }
+  block_copy(a, s.lu, L * L);
+  for (int e = threadIdx.x; e < L * L; e += blockDim.x) b[e] = make_double2(-s.g2[e].x, -s.g2[e].y);
+  for (int e = threadIdx.x; e < L; e += blockDim.x) piv[e] = s.piv[e];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const double2 z = make_double2(tot[0] / tot[2], tot[1] / tot[2]);
+    st->zeta = z;
+    st->negzeta = make_double2(-z.x, -z.y);
+    if (!zfinite(z)) atomicCAS(&st->bad, 0, 2);
+  }
+  __syncthreads();
+  if (!singular) lu_solve(a, piv, L, b, L);
+  block_copy(s.beta, b, L * L);
+}
+
+// CholeskyQR step: R = chol(G [+ shift I]), rinv = R^-1, tau <- R tau (tau = R on the first step)
+__global__ void cholqr_step_kernel(SmallPtrs s, int L, int first, double shift_coef, SolverState* st) {
+  extern __shared__ double2 sm[];
+  double2* g = sm;
+  double2* x = sm + L * L;
+  __shared__ int bad;
+  if (threadIdx.x == 0) bad = 0;
+  block_copy(g, s.g2, L * L);
+  __syncthreads();
+  if (first && shift_coef > 0.0) {
+    if (threadIdx.x == 0) {
+      double tr = 0.0;
+      for (int i = 0; i < L; ++i) tr += g[i * L + i].x;
+      const double sh = shift_coef * tr;
+      for (int i = 0; i < L; ++i) g[i * L + i].x += sh;
+    }
+    __syncthreads();
+  }
+  chol_upper(g, L, &bad);
+  tri_upper_inv(g, L, x);
+  block_copy(s.rinv, x, L * L);
+  // tau <- R tau
+  if (first) {
+    block_copy(s.tau, g, L * L);
+  } else {
+    block_copy(x, s.tau, L * L);
+    __syncthreads();
+    small_matmul<false>(g, x, s.tmp, L);
+    block_copy(s.tau, s.tmp, L * L);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0 && bad == 1) atomicExch(&st->bad, 1);
+  if (threadIdx.x == 0 && bad == 2) atomicCAS(&st->bad, 0, 2);
+}
+
+// COCG: alpha = (S^T AS)^-1 (Q^T Q); alphaxi = alpha xi   (bl_krylov.py:101-102)
+__global__ void cocg_alpha_kernel(SmallPtrs s, int L, SolverState* st) {
+  extern __shared__ double2 sm[];
+  double2* a = sm;
+  double2* b = sm + L * L;
+  double2* c = sm + 2 * L * L;
+  __shared__ int piv[kMaxL];
+  __shared__ int bad;
+  if (threadIdx.x == 0) bad = 0;
+  block_copy(a, s.g2, L * L);
+  block_copy(b, s.qq, L * L);
+  __syncthreads();
+  lu_factor(a, L, piv, &bad);
+  if (!bad) lu_solve(a, piv, L, b, L);
+  block_copy(c, s.xi, L * L);
+  __syncthreads();
+  small_matmul<false>(b, c, a, L);
+  for (int e = threadIdx.x; e < L * L; e += blockDim.x) {
+    s.alpha[e] = b[e];
+    s.negalpha[e] = make_double2(-b[e].x, -b[e].y);
+    s.alphaxi[e] = a[e];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0 && bad == 1) atomicExch(&st->bad, 1);
+  if (threadIdx.x == 0 && bad == 2) atomicCAS(&st->bad, 0, 2);
+  flag_nonfinite(b, L * L, st);
+}
+
+// COCG: xi <- tau xi; err = ||xi||_F / ||M^-1 B||_F   (bl_krylov.py:105-106)
+__global__ void cocg_xi_kernel(SmallPtrs s, int L, SolverState* st, int init) {
+  extern __shared__ double2 sm[];
+  double2* t = sm;
+  double2* x = sm + L * L;
+  double2* y = sm + 2 * L * L;
+  block_copy(t, s.tau, L * L);
+  if (init) {
+    block_copy(y, s.tau, L * L);   // xi = tau of the initial QR
+  } else {
+    block_copy(x, s.xi, L * L);
+    __syncthreads();
+    small_matmul<false>(t, x, y, L);
+  }
+  __syncthreads();
+  block_copy(s.xi, y, L * L);
+  double acc = 0.0;
+  for (int e = threadIdx.x; e < L * L; e += blockDim.x) acc += y[e].x * y[e].x + y[e].y * y[e].y;
+  __shared__ double red[256];
+  red[threadIdx.x] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double tot = 0.0;
+    for (int i = 0; i < (int)blockDim.x; ++i) tot += red[i];
+    st->err = sqrt(tot) / st->bnorm;
+    if (!isfinite(st->err)) atomicCAS(&st->bad, 0, 2);
+  }
+}
+
+// COCG: beta = (Q^T Q)^-1 (tau^T (Qn^T Qn)); Q^T Q <- Qn^T Qn   (bl_krylov.py:113-115)
+__global__ void cocg_beta_kernel(SmallPtrs s, int L, SolverState* st) {
+  extern __shared__ double2 sm[];
+  double2* a = sm;
+  double2* b = sm + L * L;
+  double2* c = sm + 2 * L * L;
+  __shared__ int piv[kMaxL];
+  __shared__ int bad;
+  if (threadIdx.x == 0) bad = 0;
+  block_copy(a, s.qq, L * L);
+  block_copy(b, s.tau, L * L);
+  block_copy(c, s.g2, L * L);
+  __syncthreads();
+  small_matmul<true>(b, c, s.tmp, L);   // tau^T (Qn^T Qn)
+  block_copy(b, s.tmp, L * L);
+  __syncthreads();
+  lu_factor(a, L, piv, &bad);
+  if (!bad) lu_solve(a, piv, L, b, L);
+  block_copy(s.beta, b, L * L);
+  block_copy(s.qq, c, L * L);
+  __syncthreads();
+  if (threadIdx.x == 0 && bad == 1) atomicExch(&st->bad, 1);
+  if (threadIdx.x == 0 && bad == 2) atomicCAS(&st->bad, 0, 2);
+}
+
+// ---- host driver ----------------------------------------------------------------
+template <typename T>
+struct Ctx {
+  const bdda_plan* plan;
+  int L;
+  int64_t n;         // rows = 3 N_occ
+  const T* ghat;
+  const int32_t* cell_map;
+  T* field;
+  T* vec[kVecs];
+  T* diag;
+  T* jpre;
+  double2* partial;
+  SmallPtrs sp;
+  SolverState* st;
+  cudaStream_t stream;
+  size_t sm2, sm3;   // dynamic smem of the small kernels (2 or 3 L x L matrices)
+};
+
+template <typename T>
+static int mvp(Ctx<T>& c, const T* in, T* out) {
+  return block_mvp_impl<T>(c.plan, c.L, c.ghat, c.cell_map, c.diag, c.jpre, in, out, c.field, c.stream);
+}
+
+template <typename T>
+static int gram2(Ctx<T>& c, bool conj, const T* A, const T* B0, const T* B1, double2* out) {
+  GramArgs g;
+  g.n = c.n; g.L = c.L; g.nB = B1 ? 2 : 1; g.A = A; g.B[0] = B0; g.B[1] = B1; g.partial = c.partial;
+  return gram<T>(g, conj, out, c.stream);
+}
+
+template <typename T>
+static int upd(Ctx<T>& c, T* out, const T* Y0, const double2* a0, const T* Y1, const double2* a1,
+               const T* X1, const T* X2, const double2* c2, const double2* M, bool norm) {
+  UpdateArgs u;
+  u.n = c.n; u.L = c.L;
+  u.Y0 = Y0; u.a0 = a0; u.Y1 = Y1; u.a1 = a1; u.X1 = X1; u.X2 = X2; u.c2 = c2; u.M = M;
+  u.out = out;
+  u.norm_partial = norm ? reinterpret_cast<double*>(c.partial) : nullptr;
+  return update<T>(u, c.stream);
+}
+
+template <typename T>
+static int read_state(Ctx<T>& c, double* err, int* bad) {
+  SolverState h;
+  BDDA_CUDA_TRY(cudaMemcpyAsync(&h, c.st, sizeof(h), cudaMemcpyDeviceToHost, c.stream));
+  BDDA_CUDA_TRY(cudaStreamSynchronize(c.stream));
+  *err = h.err;
+  *bad = h.bad;
+  return BDDA_OK;
+}
+
+#define TRY(expr)                 \
+  do {                            \
+    int s_ = (expr);              \
+    if (s_ != BDDA_OK) return s_; \
+  } while (0)
+
+// Block-BiCGSTAB (bl_krylov.py:121-187).  vec: 0 X, 1 R, 2 P, 3 R0, 4 V, 5 T, 6 Z, 7 Bj
+template <typename T>
+static int bicgstab_core(Ctx<T>& c, bool has_x0, double tol, int itermax, int* iter_fin,
+                         double* err_fin, double* hist) {
+  T *X = c.vec[0], *R = c.vec[1], *P = c.vec[2], *R0 = c.vec[3], *V = c.vec[4], *Tt = c.vec[5],
+    *Z = c.vec[6], *Bj = c.vec[7];
+  const int L = c.L;
+  double* dot_partial = reinterpret_cast<double*>(c.partial) + 2 * (size_t)kMaxL * kMaxL * kRedBlocks;
+  // R = M^-1 B and ||M^-1 B|| (bl_krylov.py:149-153)
+  TRY(upd<T>(c, R, Bj, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, true));
+  norm_kernel<<<1, 256, 0, c.stream>>>(reinterpret_cast<double*>(c.partial), kRedBlocks, c.st, 1);
+  count_launch();
+  BDDA_CUDA_TRY(cudaGetLastError());
+  if (has_x0) {   // R = M^-1 (B - A X0)
+    TRY(mvp<T>(c, X, V));
+    TRY(upd<T>(c, R, Bj, nullptr, V, c.sp.r, nullptr, nullptr, nullptr, nullptr, false));
+  }
+  TRY(upd<T>(c, P, R, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, false));
+  TRY(upd<T>(c, R0, R, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, false));
+  *iter_fin = 0;
+  *err_fin = INFINITY;
+  double err = INFINITY;
+  for (int k = 0; k < itermax; ++k) {
+    TRY(mvp<T>(c, P, V));                                   // V = M^-1 A P
+    TRY(gram2<T>(c, true, R0, V, R, c.sp.g2));              // R0^H V, R0^H R
+    bicg_alpha_kernel<<<1, 256, c.sm2, c.stream>>>(c.sp, L, c.st);
+    count_launch();
+    BDDA_CUDA_TRY(cudaGetLastError());
+    TRY(upd<T>(c, Tt, R, nullptr, nullptr, nullptr, V, nullptr, nullptr, c.sp.negalpha, false));  // T = R - V alpha
+    TRY(mvp<T>(c, Tt, Z));                                  // Z = M^-1 A T
+    TRY(gram2<T>(c, true, R0, Z, nullptr, c.sp.g2));        // R0^H Z
+    DotArgs d;
+    d.n = c.n * L; d.A = Z; d.B = Tt; d.partial = dot_partial;
+    TRY(dots<T>(d, c.stream));                              // tr(Z^H T), tr(Z^H Z)
+    bicg_zeta_beta_kernel<<<1, 256, c.sm2, c.stream>>>(c.sp, L, dot_partial, kRedBlocks, c.st);
+    count_launch();
+    BDDA_CUDA_TRY(cudaGetLastError());
+    TRY(upd<T>(c, X, X, nullptr, Tt, &c.st->zeta, P, nullptr, nullptr, c.sp.alpha, false));  // X += P alpha + zeta T
+    TRY(upd<T>(c, R, Tt, nullptr, Z, &c.st->negzeta, nullptr, nullptr, nullptr, nullptr, true));  // R = T - zeta Z
+    norm_kernel<<<1, 256, 0, c.stream>>>(reinterpret_cast<double*>(c.partial), kRedBlocks, c.st, 0);
+    count_launch();
+    BDDA_CUDA_TRY(cudaGetLastError());
+    int bad = 0;
+    TRY(read_state(c, &err, &bad));
+    if (bad == 1) return BDDA_BREAKDOWN;
+    if (hist) hist[k] = err;
+    *iter_fin = k;
+    *err_fin = err;
+    if (bad == 2) return BDDA_NOT_CONVERGED;   // NaN/Inf reached: stop, reported as not converged
+    if (err < tol) return BDDA_OK;
+    // P = R + (P - zeta V) beta
+    TRY(upd<T>(c, P, R, nullptr, nullptr, nullptr, P, V, &c.st->negzeta, c.sp.beta, false));
+  }
+  return BDDA_NOT_CONVERGED;
+}
+
+// Shifted CholeskyQR3: Q R = W with R accumulated into sp.tau; the first step
+// adds 11 (n L + L (L+1)) u tr(W^H W) to the diagonal so that it cannot fail
+// for numerically rank-deficient W.  Writes sa, sb; Q ends in sa.
+template <typename T>
+static int cholqr3(Ctx<T>& c, const T* W, T* sa, T* sb, T** qout) {
+  const double u = 1.1102230246251565e-16;
+  const double shift = 11.0 * ((double)c.n * c.L + (double)c.L * (c.L + 1)) * u;
+  const T* in = W;
+  T* outs[3] = {sa, sb, sa};
+  for (int step = 0; step < 3; ++step) {
+    TRY(gram2<T>(c, true, in, in, nullptr, c.sp.g2));
+    cholqr_step_kernel<<<1, 256, c.sm2, c.stream>>>(c.sp, c.L, step == 0, step == 0 ? shift : 0.0, c.st);
+    count_launch();
+    BDDA_CUDA_TRY(cudaGetLastError());
+    TRY(upd<T>(c, outs[step], nullptr, nullptr, nullptr, nullptr, in, nullptr, nullptr, c.sp.rinv, false));
+    in = outs[step];
+  }
+  *qout = outs[2];
+  return BDDA_OK;
+}
+
+// Block-COCG-rq (bl_krylov.py:58-118).  vec: 0 X, 1-2-3 rotating Q / QR scratch,
+// 4 S, 5 AS, 6 W, 7 Bj
+template <typename T>
+static int cocg_core(Ctx<T>& c, bool has_x0, double tol, int itermax, int* iter_fin, double* err_fin,
+                     double* hist) {
+  T *X = c.vec[0], *S = c.vec[4], *AS = c.vec[5], *W = c.vec[6], *Bj = c.vec[7];
+  T* rot[3] = {c.vec[1], c.vec[2], c.vec[3]};   // rot[0] holds Q, rot[1..2] are QR scratch
+  const int L = c.L;
+  // ||M^-1 B|| (bl_krylov.py:87-88); W = M^-1 (B - A X0)
+  TRY(upd<T>(c, W, Bj, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, true));
+  norm_kernel<<<1, 256, 0, c.stream>>>(reinterpret_cast<double*>(c.partial), kRedBlocks, c.st, 1);
+  count_launch();
+  BDDA_CUDA_TRY(cudaGetLastError());
+  if (has_x0) {
+    TRY(mvp<T>(c, X, AS));
+    TRY(upd<T>(c, W, Bj, nullptr, AS, c.sp.r, nullptr, nullptr, nullptr, nullptr, false));
+  }
+  // Q, xi = qr(W)   (bl_krylov.py:92)
+  T* q = nullptr;
+  TRY(cholqr3<T>(c, W, rot[1], rot[2], &q));
+  std::swap(rot[0], rot[1]);               // Q now in rot[0]
+  cocg_xi_kernel<<<1, 256, c.sm3, c.stream>>>(c.sp, L, c.st, 1);
+  count_launch();
+  BDDA_CUDA_TRY(cudaGetLastError());
+  TRY(upd<T>(c, S, rot[0], nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, false));
+  TRY(gram2<T>(c, false, rot[0], rot[0], nullptr, c.sp.qq));
+  *iter_fin = 0;
+  *err_fin = INFINITY;
+  double err = INFINITY;
+  for (int k = 0; k < itermax; ++k) {
+    TRY(mvp<T>(c, S, AS));
+    TRY(gram2<T>(c, false, S, AS, nullptr, c.sp.g2));
+    cocg_alpha_kernel<<<1, 256, c.sm3, c.stream>>>(c.sp, L, c.st);
+    count_launch();
+    BDDA_CUDA_TRY(cudaGetLastError());
+    TRY(upd<T>(c, X, X, nullptr, nullptr, nullptr, S, nullptr, nullptr, c.sp.alphaxi, false));
+    TRY(upd<T>(c, W, rot[0], nullptr, nullptr, nullptr, AS, nullptr, nullptr, c.sp.negalpha, false));
+    TRY(cholqr3<T>(c, W, rot[1], rot[2], &q));   // Qnew in rot[1], tau in sp.tau
+    cocg_xi_kernel<<<1, 256, c.sm3, c.stream>>>(c.sp, L, c.st, 0);
+    count_launch();
+    BDDA_CUDA_TRY(cudaGetLastError());
+    int bad = 0;
+    TRY(read_state(c, &err, &bad));
+    if (bad == 1) return BDDA_BREAKDOWN;
+    if (hist) hist[k] = err;
+    *iter_fin = k;
+    *err_fin = err;
+    if (bad == 2) return BDDA_NOT_CONVERGED;
+    if (err < tol) return BDDA_OK;
+    TRY(gram2<T>(c, false, rot[1], rot[1], nullptr, c.sp.g2));
+    cocg_beta_kernel<<<1, 256, c.sm3, c.stream>>>(c.sp, L, c.st);
+    count_launch();
+    BDDA_CUDA_TRY(cudaGetLastError());
+    TRY(upd<T>(c, S, rot[1], nullptr, nullptr, nullptr, S, nullptr, nullptr, c.sp.beta, false));
+    std::swap(rot[0], rot[1]);             // Q <- Qnew
+  }
+  return BDDA_NOT_CONVERGED;
+}
+
+__global__ void constants_kernel(SmallPtrs s) {
+  if (threadIdx.x == 0) s.r[0] = make_double2(-1.0, 0.0);
+}
+
+template <typename K>
+static int allow_smem(K kern, size_t bytes) {
+  BDDA_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  return BDDA_OK;
+}
+
+template <typename T>
+static int run_solver(int solver, const bdda_plan* p, int L, int n_occ, const void* ghat,
+                      const int32_t* cell_map, const double2* diag, const double2* B, const double2* X0,
+                      double tol, int itermax, double2* Xout, int* iter_fin, double* err_fin,
+                      double* hist, void* work, size_t work_bytes, cudaStream_t st) {
+  const int prec = std::is_same<T, double2>::value ? BDDA_C128 : BDDA_C64;
+  const Layout o = layout(p, prec, L, n_occ);
+  if (work_bytes < o.total) return BDDA_NO_WORKSPACE;
+  unsigned char* w = static_cast<unsigned char*>(work);
+  Ctx<T> c;
+  c.plan = p;
+  c.L = L;
+  c.n = 3 * (int64_t)n_occ;
+  c.ghat = static_cast<const T*>(ghat);
+  c.cell_map = cell_map;
+  c.field = reinterpret_cast<T*>(w + o.field);
+  for (int v = 0; v < kVecs; ++v) c.vec[v] = reinterpret_cast<T*>(w + o.vec[v]);
+  c.diag = reinterpret_cast<T*>(w + o.diag);
+  c.jpre = reinterpret_cast<T*>(w + o.jpre);
+  c.partial = reinterpret_cast<double2*>(w + o.partial);
+  c.sp = small_ptrs(w + o.small);
+  c.st = reinterpret_cast<SolverState*>(w + o.state);
+  c.stream = st;
+  c.sm2 = (size_t)2 * L * L * sizeof(double2);
+  c.sm3 = (size_t)3 * L * L * sizeof(double2);
+  TRY(allow_smem(bicg_alpha_kernel, c.sm2));
+  TRY(allow_smem(bicg_zeta_beta_kernel, c.sm2));
+  TRY(allow_smem(cholqr_step_kernel, c.sm2));
+  TRY(allow_smem(cocg_alpha_kernel, c.sm3));
+  TRY(allow_smem(cocg_xi_kernel, c.sm3));
+  TRY(allow_smem(cocg_beta_kernel, c.sm3));
+  BDDA_CUDA_TRY(cudaMemsetAsync(c.st, 0, sizeof(SolverState), st));
+  constants_kernel<<<1, 32, 0, st>>>(c.sp);
+  count_launch();
+  prepare_kernel<T><<<kRedBlocks, 256, 0, st>>>(diag, B, c.n, L, c.diag, c.jpre, c.vec[7]);
+  count_launch();
+  BDDA_CUDA_TRY(cudaGetLastError());
+  if (X0) {
+    convert_in_kernel<T><<<kRedBlocks, 256, 0, st>>>(X0, c.vec[0], c.n * L);
+    count_launch();
+    BDDA_CUDA_TRY(cudaGetLastError());
+  } else {
+    BDDA_CUDA_TRY(cudaMemsetAsync(c.vec[0], 0, (size_t)c.n * L * sizeof(T), st));
+  }
+  const int status = solver == BDDA_COCG_RQ
+                         ? cocg_core<T>(c, X0 != nullptr, tol, itermax, iter_fin, err_fin, hist)
+                         : bicgstab_core<T>(c, X0 != nullptr, tol, itermax, iter_fin, err_fin, hist);
+  if (status == BDDA_OK || status == BDDA_NOT_CONVERGED) {
+    convert_out_kernel<T><<<kRedBlocks, 256, 0, st>>>(c.vec[0], Xout, c.n * L);
+    count_launch();
+    BDDA_CUDA_TRY(cudaGetLastError());
+  }
+  return status;
+}
+
+}  // namespace bdda
+
+using namespace bdda;
+
+extern "C" {
+
+size_t bdda_solver_workspace_bytes(const bdda_plan* p, int solver, int prec, int L, int n_occ) {
+  if (!p || L < 1 || L > kMaxL || n_occ < 1 || (solver != BDDA_BICGSTAB && solver != BDDA_COCG_RQ) ||
+      (prec != BDDA_C128 && prec != BDDA_C64))
+    return 0;
+  return layout(p, prec, L, n_occ).total;
+}
+
+int bdda_solve(const bdda_plan* p, int solver, int prec, int L, int n_occ, const void* ghat,
+               const int32_t* cell_map, const void* diag, const void* B, const void* X0, double tol,
+               int itermax, void* X, int* iter_fin, double* err_fin, double* history, void* work,
+               size_t work_bytes, void* stream) {
+  if (!p || L < 1 || L > kMaxL || n_occ < 1 || !ghat || !cell_map || !diag || !B || !X || !iter_fin ||
+      !err_fin || itermax < 0 || !(tol == tol))
+    return BDDA_BAD_ARG;
+  if (solver != BDDA_BICGSTAB && solver != BDDA_COCG_RQ) return BDDA_BAD_ARG;
+  if (!work || !p->dev_tables) return BDDA_NO_WORKSPACE;
+  *iter_fin = 0;
+  *err_fin = INFINITY;
+  if (itermax == 0) {   // the reference returns X = 0 without iterating
+    BDDA_CUDA_TRY(cudaMemsetAsync(X, 0, (size_t)3 * n_occ * L * sizeof(double2), (cudaStream_t)stream));
+    return BDDA_NOT_CONVERGED;
+  }
+  const cudaStream_t st = (cudaStream_t)stream;
+  if (prec == BDDA_C128)
+    return run_solver<double2>(solver, p, L, n_occ, ghat, cell_map, static_cast<const double2*>(diag),
+                               static_cast<const double2*>(B), static_cast<const double2*>(X0), tol,
+                               itermax, static_cast<double2*>(X), iter_fin, err_fin, history, work,
+                               work_bytes, st);
+  if (prec == BDDA_C64)
+    return run_solver<float2>(solver, p, L, n_occ, ghat, cell_map, static_cast<const double2*>(diag),
+                              static_cast<const double2*>(B), static_cast<const double2*>(X0), tol,
+                              itermax, static_cast<double2*>(X), iter_fin, err_fin, history, work,
+                              work_bytes, st);
+  return BDDA_BAD_ARG;
+}
+
+int bdda_bicgstab(const bdda_plan* p, int prec, int L, int n_occ, const void* ghat,
+                  const int32_t* cell_map, const void* diag, const void* B, const void* X0, double tol,
+                  int itermax, void* X, int* iter_fin, double* err_fin, double* history, void* work,
+                  size_t work_bytes, void* stream) {
+  return bdda_solve(p, BDDA_BICGSTAB, prec, L, n_occ, ghat, cell_map, diag, B, X0, tol, itermax, X,
+                    iter_fin, err_fin, history, work, work_bytes, stream);
+}
+
+int bdda_cocg_rq(const bdda_plan* p, int prec, int L, int n_occ, const void* ghat,
+                 const int32_t* cell_map, const void* diag, const void* B, const void* X0, double tol,
+                 int itermax, void* X, int* iter_fin, double* err_fin, double* history, void* work,
+                 size_t work_bytes, void* stream) {
+  return bdda_solve(p, BDDA_COCG_RQ, prec, L, n_occ, ghat, cell_map, diag, B, X0, tol, itermax, X,
+                    iter_fin, err_fin, history, work, work_bytes, stream);
+}
+
+}  // extern "C"

@@ -50,6 +50,11 @@ enum bdda_status {
   BDDA_CUDA_ERROR = 6     /* a CUDA runtime call failed */
 };
 
+enum bdda_solver_kind {
+  BDDA_BICGSTAB = 0, /* block-BiCGSTAB, bl_krylov/bl_krylov.py:121 */
+  BDDA_COCG_RQ = 1   /* block-COCG-rq,  bl_krylov/bl_krylov.py:58 */
+};
+
 enum bdda_precision {
   BDDA_C128 = 0, /* complex128 end to end */
   BDDA_C64 = 1   /* complex64 storage, FP32 arithmetic */
@@ -108,6 +113,70 @@ int bdda_fft_mvp(const bdda_plan* plan, int prec, int L, const void* ghat, const
 int bdda_block_mvp(const bdda_plan* plan, int prec, int L, const void* ghat,
                    const int32_t* cell_map, const void* diag, const void* jpre, const void* S,
                    void* out, void* work, void* stream);
+
+/* ---- block Krylov solvers -----------------------------------------------------
+ * Solve A X = B with Jacobi left preconditioning, M = diag(A): iterate on
+ * M^-1 A X = M^-1 B until ||R||_F / ||M^-1 B||_F < tol (a single global
+ * Frobenius criterion over the L columns, bl_krylov.py:106,177) or itermax
+ * iterations.  diag (3 N_occ) c128 is DIAG_A; B, X0 (nullable = zero start)
+ * and X are (3 N_occ, L) c128.  prec selects the storage/arithmetic of the
+ * Krylov vectors and of the product (ghat must be in that precision); the
+ * L x L Gram matrices, solves and QR factors are always FP64.
+ * iter_fin is the 0-based index of the last iteration, err_fin its relative
+ * residual (reference semantics); history (nullable, itermax doubles, host)
+ * receives the residual of every iteration.  L <= 64.
+ * Returns BDDA_OK (converged), BDDA_NOT_CONVERGED (itermax reached, or the
+ * iteration produced non-finite values: err_fin is then NaN/Inf), or
+ * BDDA_BREAKDOWN (exactly singular L x L system: numpy's LinAlgError).
+ * The stream is synchronised once per iteration to read the residual. */
+size_t bdda_solver_workspace_bytes(const bdda_plan* plan, int solver, int prec, int L, int n_occ);
+int bdda_solve(const bdda_plan* plan, int solver, int prec, int L, int n_occ, const void* ghat,
+               const int32_t* cell_map, const void* diag, const void* B, const void* X0, double tol,
+               int itermax, void* X, int* iter_fin, double* err_fin, double* history, void* work,
+               size_t work_bytes, void* stream);
+/* replaces bl_krylov/bl_krylov.py:121 bl_bicgstab_jacobi_mvp_fft */
+int bdda_bicgstab(const bdda_plan* plan, int prec, int L, int n_occ, const void* ghat,
+                  const int32_t* cell_map, const void* diag, const void* B, const void* X0,
+                  double tol, int itermax, void* X, int* iter_fin, double* err_fin,
+                  double* history, void* work, size_t work_bytes, void* stream);
+/* replaces bl_krylov/bl_krylov.py:58 bl_cocg_rq_jacobi_mvp_fft */
+int bdda_cocg_rq(const bdda_plan* plan, int prec, int L, int n_occ, const void* ghat,
+                 const int32_t* cell_map, const void* diag, const void* B, const void* X0,
+                 double tol, int itermax, void* X, int* iter_fin, double* err_fin,
+                 double* history, void* work, size_t work_bytes, void* stream);
+
+/* ---- physics around the solve --------------------------------------------------
+ * Homogeneous particle, per-axis index m_p_xyz = (re x, im x, re y, im y, re z, im z):
+ * eps_r = m_p^2 / m_m^2, Clausius-Mossotti polarizability with the CR2009
+ * correction, diag = 1 / alpha ordered [x0 y0 z0 x1 ...] (3 N_occ c128);
+ * eper_r (nullable) receives eps_r in the same order.
+ * replaces bl_dda/scatterer.py:137-148 */
+int bdda_polarizability(int n_occ, const double m_p_xyz[6], double m_m, double lf, double k, void* diag,
+                        void* eper_r, void* stream);
+/* B[3n + c, l] = e0[l, c] exp(i k u_inc[l] . pos[n]); pos (N_occ, 3) and
+ * u_inc (L, 3) double, e0 (L, 3) c128, all on the device.
+ * replaces bl_dda/scatterer.py:153-161 */
+int bdda_incident_rhs(int n_occ, int L, double k, const double* pos, const double* u_inc, const void* e0,
+                      void* B, void* stream);
+/* Per orientation, from the solution X (3 N_occ, L): out (L, 12) doubles =
+ * C_abs, C_ext, S_fw_theta (re, im), S_fw_phi, S_bk_theta, S_bk_phi, S_bk.
+ * vec (L, 21) doubles = u_inc, u_fw, theta_fw, phi_fw, u_bk, theta_bk, phi_bk
+ * (particle frame); e0 (L, 3) c128; eper_r (3 N_occ) c128; absorbing = mean
+ * Im eps_r >= 1e-12 (else C_abs = 0, scatterer.py:189).
+ * replaces bl_dda/scatterer.py:182-227 */
+size_t bdda_observables_workspace_bytes(int L);
+int bdda_observables(int n_occ, int L, double k, double lf, int absorbing, const double* pos,
+                     const void* eper_r, const void* X, const double* vec, const void* e0, double* out,
+                     void* work, void* stream);
+
+/* ---- instrumentation (no counterpart in the reference) -------------------------
+ * Number of kernels this library has launched in the process.  With
+ * profiling on, every block MVP records CUDA events around its five passes;
+ * bdda_profile_read waits for them and returns the summed milliseconds of
+ * each pass and the number of products.  Enabling clears earlier records. */
+unsigned long long bdda_launch_count(void);
+int bdda_profile_enable(int on);
+int bdda_profile_read(double pass_ms[5], long long* n_mvp);
 
 #ifdef __cplusplus
 }
