@@ -322,16 +322,65 @@ def run_reference(args, rank, world):
             "e2e": {"value": v, "unit": "orientations/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
+def run_mvp_only(args):
+    """Block MVPs of the workload only (profiling case); prints per-pass timings."""
+    import torch
+    from bdda_b200 import _lib
+    from bdda_b200.runtime import TORCH_DTYPE, GreenTensor, Occupancy, Plan, precision_code, ptr, stream_ptr
+    geo, _ = load_workload(args.L)
+    lib = _lib.load()
+    prec = precision_code("c128" if args.form == "fp64" else "c64")
+    plan = Plan(geo["lattice_n"])
+    k = 2 * np.pi * float(geo["m_m"]) / float(geo["wl_0"])
+    green = GreenTensor(plan, geo["lattice_lf"], k)
+    occ = Occupancy(plan, geo["address"])
+    dt = TORCH_DTYPE[prec]
+    gen = torch.Generator(device="cuda").manual_seed(0)
+    S = torch.randn((3 * occ.n_occ, args.L), dtype=dt, device="cuda", generator=gen)
+    out = torch.empty_like(S)
+    diag = torch.full((3 * occ.n_occ,), 2.0 + 0.1j, dtype=dt, device="cuda")
+    jpre = 1.0 / diag
+    work = green.workspace(prec, args.L)
+    gh = green.ghat(prec)
+
+    def mvp():
+        _lib.check(lib.bdda_block_mvp(plan.handle, prec, args.L, ptr(gh), ptr(occ.cell_map), ptr(diag),
+                                      ptr(jpre), ptr(S), ptr(out), ptr(work), stream_ptr()), "mvp")
+    for _ in range(args.warmup):
+        mvp()
+    torch.cuda.synchronize()
+    lib.bdda_profile_enable(1)
+    for _ in range(args.steps):
+        mvp()
+    torch.cuda.synchronize()
+    pass_ms = (_lib.C.c_double * 5)()
+    nm = _lib.C.c_longlong(0)
+    lib.bdda_profile_read(pass_ms, _lib.C.byref(nm))
+    lib.bdda_profile_enable(0)
+    s = 16 if prec == _lib.C128 else 8
+    pb = mvp_pass_bytes(plan.n, plan.m, occ.n_occ, args.L, s)
+    per = [pass_ms[i] / max(1, nm.value) for i in range(5)]
+    print(json.dumps({"mvp_only": True, "L": args.L, "form": args.form, "grid": plan.m,
+                      "radices": [plan.radices(a) for a in range(3)], "mvp_ms": round(sum(per), 3),
+                      "GB/s": round(sum(pb) / (sum(per) * 1e-3) / 1e9, 1),
+                      "passes_ms": [round(x, 3) for x in per],
+                      "passes_GBs": [round(b / (t * 1e-3) / 1e9, 1) for b, t in zip(pb, per)]}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="bdda", choices=["bdda", "reference"])
-    ap.add_argument("--form", default="fp64", choices=["fp64"])
+    ap.add_argument("--form", default="fp64", choices=["fp64", "fp32"])
     ap.add_argument("--L", type=int, default=64)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--mvp-only", action="store_true", help="time block MVPs of the workload only")
     args = ap.parse_args()
+    if args.mvp_only:
+        run_mvp_only(args)
+        return
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     local_rank = int(os.environ.get("LOCAL_RANK", 0))

@@ -32,6 +32,9 @@ _pi = C.POINTER(C.c_int)
 PROTOTYPES = {
     "bdda_status_string": (C.c_char_p, [_i]),
     "bdda_version": (_i, []),
+    "bdda_tune_set": (_i, [_i, _i, _sz, _i]),
+    "bdda_tune_get": (_i, [_i, _i, C.POINTER(_sz), _pi]),
+    "bdda_tune_fixed": (_i, [_i]),
     "bdda_plan_create": (_i, [_pi, _pi, C.POINTER(_vp)]),
     "bdda_plan_destroy": (None, [_vp]),
     "bdda_plan_grid": (_i, [_vp, _pi]),

@@ -46,29 +46,82 @@ template <bool INV, typename T> __device__ __forceinline__ T mul_mi(T a) {
   return INV ? mkc<T>(-a.y, a.x) : mkc<T>(a.y, -a.x);
 }
 
-// cos / sin of 2*pi*j/R for the odd radices (values from the definition,
-// 25 significant digits, rounded by the compiler to the working precision)
+// cos / sin of 2*pi*j/R for the odd and composite radices (values from the
+// definition, 25 significant digits, rounded by the compiler to the working
+// precision)
 template <int R> __device__ __forceinline__ constexpr double root_cos(int j);
 template <int R> __device__ __forceinline__ constexpr double root_sin(int j);
-template <> __device__ __forceinline__ constexpr double root_cos<3>(int j) { return j == 0 ? 1.0 : -0.5; }
+template <> __device__ __forceinline__ constexpr double root_cos<3>(int j) {
+  constexpr double t[3] = {1.000000000000000000000000, -0.5000000000000000000000000, -0.5000000000000000000000000};
+  return t[j];
+}
 template <> __device__ __forceinline__ constexpr double root_sin<3>(int j) {
-  return j == 0 ? 0.0 : (j == 1 ? 0.8660254037844386467637232 : -0.8660254037844386467637232);
+  constexpr double t[3] = {0.0, 0.8660254037844386467637232, -0.8660254037844386467637232};
+  return t[j];
 }
 template <> __device__ __forceinline__ constexpr double root_cos<5>(int j) {
-  return j == 0 ? 1.0 : (j == 1 || j == 4) ? 0.3090169943749474241022934 : -0.8090169943749474241022934;
+  constexpr double t[5] = {1.000000000000000000000000, 0.3090169943749474241022934, -0.8090169943749474241022934, -0.8090169943749474241022934, 0.3090169943749474241022934};
+  return t[j];
 }
 template <> __device__ __forceinline__ constexpr double root_sin<5>(int j) {
-  return j == 0 ? 0.0 : j == 1 ? 0.9510565162951535721164393 : j == 2 ? 0.587785252292473129168706
-       : j == 3 ? -0.587785252292473129168706 : -0.9510565162951535721164393;
+  constexpr double t[5] = {0.0, 0.9510565162951535721164393, 0.5877852522924731291687060, -0.5877852522924731291687060, -0.9510565162951535721164393};
+  return t[j];
+}
+template <> __device__ __forceinline__ constexpr double root_cos<6>(int j) {
+  constexpr double t[6] = {1.000000000000000000000000, 0.5000000000000000000000000, -0.5000000000000000000000000, -1.000000000000000000000000, -0.5000000000000000000000000, 0.5000000000000000000000000};
+  return t[j];
+}
+template <> __device__ __forceinline__ constexpr double root_sin<6>(int j) {
+  constexpr double t[6] = {0.0, 0.8660254037844386467637232, 0.8660254037844386467637232, 0.0, -0.8660254037844386467637232, -0.8660254037844386467637232};
+  return t[j];
 }
 template <> __device__ __forceinline__ constexpr double root_cos<7>(int j) {
-  return j == 0 ? 1.0 : (j == 1 || j == 6) ? 0.6234898018587335305250049
-       : (j == 2 || j == 5) ? -0.2225209339563144042889026 : -0.9009688679024191262361023;
+  constexpr double t[7] = {1.000000000000000000000000, 0.6234898018587335305250049, -0.2225209339563144042889026, -0.9009688679024191262361023, -0.9009688679024191262361023, -0.2225209339563144042889026, 0.6234898018587335305250049};
+  return t[j];
 }
 template <> __device__ __forceinline__ constexpr double root_sin<7>(int j) {
-  return j == 0 ? 0.0 : j == 1 ? 0.7818314824680298087084445 : j == 2 ? 0.9749279121818236070181317
-       : j == 3 ? 0.4338837391175581204757683 : j == 4 ? -0.4338837391175581204757683
-       : j == 5 ? -0.9749279121818236070181317 : -0.7818314824680298087084445;
+  constexpr double t[7] = {0.0, 0.7818314824680298087084445, 0.9749279121818236070181317, 0.4338837391175581204757683, -0.4338837391175581204757683, -0.9749279121818236070181317, -0.7818314824680298087084445};
+  return t[j];
+}
+template <> __device__ __forceinline__ constexpr double root_cos<9>(int j) {
+  constexpr double t[9] = {1.000000000000000000000000, 0.7660444431189780352023927, 0.1736481776669303488517166, -0.5000000000000000000000000, -0.9396926207859083840541093, -0.9396926207859083840541093, -0.5000000000000000000000000, 0.1736481776669303488517166, 0.7660444431189780352023927};
+  return t[j];
+}
+template <> __device__ __forceinline__ constexpr double root_sin<9>(int j) {
+  constexpr double t[9] = {0.0, 0.6427876096865393263226434, 0.9848077530122080593667430, 0.8660254037844386467637232, 0.3420201433256687330440996, -0.3420201433256687330440996, -0.8660254037844386467637232, -0.9848077530122080593667430, -0.6427876096865393263226434};
+  return t[j];
+}
+template <> __device__ __forceinline__ constexpr double root_cos<10>(int j) {
+  constexpr double t[10] = {1.000000000000000000000000, 0.8090169943749474241022934, 0.3090169943749474241022934, -0.3090169943749474241022934, -0.8090169943749474241022934, -1.000000000000000000000000, -0.8090169943749474241022934, -0.3090169943749474241022934, 0.3090169943749474241022934, 0.8090169943749474241022934};
+  return t[j];
+}
+template <> __device__ __forceinline__ constexpr double root_sin<10>(int j) {
+  constexpr double t[10] = {0.0, 0.5877852522924731291687060, 0.9510565162951535721164393, 0.9510565162951535721164393, 0.5877852522924731291687060, 0.0, -0.5877852522924731291687060, -0.9510565162951535721164393, -0.9510565162951535721164393, -0.5877852522924731291687060};
+  return t[j];
+}
+template <> __device__ __forceinline__ constexpr double root_cos<12>(int j) {
+  constexpr double t[12] = {1.000000000000000000000000, 0.8660254037844386467637232, 0.5000000000000000000000000, 0.0, -0.5000000000000000000000000, -0.8660254037844386467637232, -1.000000000000000000000000, -0.8660254037844386467637232, -0.5000000000000000000000000, 0.0, 0.5000000000000000000000000, 0.8660254037844386467637232};
+  return t[j];
+}
+template <> __device__ __forceinline__ constexpr double root_sin<12>(int j) {
+  constexpr double t[12] = {0.0, 0.5000000000000000000000000, 0.8660254037844386467637232, 1.000000000000000000000000, 0.8660254037844386467637232, 0.5000000000000000000000000, 0.0, -0.5000000000000000000000000, -0.8660254037844386467637232, -1.000000000000000000000000, -0.8660254037844386467637232, -0.5000000000000000000000000};
+  return t[j];
+}
+template <> __device__ __forceinline__ constexpr double root_cos<14>(int j) {
+  constexpr double t[14] = {1.000000000000000000000000, 0.9009688679024191262361023, 0.6234898018587335305250049, 0.2225209339563144042889026, -0.2225209339563144042889026, -0.6234898018587335305250049, -0.9009688679024191262361023, -1.000000000000000000000000, -0.9009688679024191262361023, -0.6234898018587335305250049, -0.2225209339563144042889026, 0.2225209339563144042889026, 0.6234898018587335305250049, 0.9009688679024191262361023};
+  return t[j];
+}
+template <> __device__ __forceinline__ constexpr double root_sin<14>(int j) {
+  constexpr double t[14] = {0.0, 0.4338837391175581204757683, 0.7818314824680298087084445, 0.9749279121818236070181317, 0.9749279121818236070181317, 0.7818314824680298087084445, 0.4338837391175581204757683, 0.0, -0.4338837391175581204757683, -0.7818314824680298087084445, -0.9749279121818236070181317, -0.9749279121818236070181317, -0.7818314824680298087084445, -0.4338837391175581204757683};
+  return t[j];
+}
+template <> __device__ __forceinline__ constexpr double root_cos<16>(int j) {
+  constexpr double t[16] = {1.000000000000000000000000, 0.9238795325112867561281832, 0.7071067811865475244008444, 0.3826834323650897717284600, 0.0, -0.3826834323650897717284600, -0.7071067811865475244008444, -0.9238795325112867561281832, -1.000000000000000000000000, -0.9238795325112867561281832, -0.7071067811865475244008444, -0.3826834323650897717284600, 0.0, 0.3826834323650897717284600, 0.7071067811865475244008444, 0.9238795325112867561281832};
+  return t[j];
+}
+template <> __device__ __forceinline__ constexpr double root_sin<16>(int j) {
+  constexpr double t[16] = {0.0, 0.3826834323650897717284600, 0.7071067811865475244008444, 0.9238795325112867561281832, 1.000000000000000000000000, 0.9238795325112867561281832, 0.7071067811865475244008444, 0.3826834323650897717284600, 0.0, -0.3826834323650897717284600, -0.7071067811865475244008444, -0.9238795325112867561281832, -1.000000000000000000000000, -0.9238795325112867561281832, -0.7071067811865475244008444, -0.3826834323650897717284600};
+  return t[j];
 }
 
 // ---- small DFTs on registers: y_q = sum_p v_p exp(-+2 pi i p q / R) ----------
@@ -131,45 +184,58 @@ template <int R, bool INV, typename T> __device__ __forceinline__ void dft_odd(T
   for (int q = 0; q < R; ++q) v[q] = y[q];
 }
 
+template <int R, bool INV, typename T> __device__ __forceinline__ void dft(T* v);
+
+// v *= exp(-+2 pi i m / R) for a compile-time-known m (after unrolling);
+// the four quarter turns are exact swaps / negations
+template <int R, bool INV, typename T> __device__ __forceinline__ T twiddle_const(T v, int m) {
+  typedef typename real_of<T>::type F;
+  m %= R;
+  if (m == 0) return v;
+  if (4 * m == R) return mul_mi<INV>(v);
+  if (2 * m == R) return mkc<T>(-v.x, -v.y);
+  if (4 * m == 3 * R) return mul_mi<!INV>(v);
+  const F c = F(root_cos<R>(m));
+  const F s = INV ? F(root_sin<R>(m)) : F(-root_sin<R>(m));
+  return mkc<T>(v.x * c - v.y * s, v.x * s + v.y * c);
+}
+
+// Cooley-Tukey on registers for R = A * B: x[n1 + A n2] -> X[k2 + B k1]
+template <int A, int B, bool INV, typename T> __device__ __forceinline__ void dft_ab(T* v) {
+  constexpr int R = A * B;
+  T u[R];
+#pragma unroll
+  for (int n1 = 0; n1 < A; ++n1) {
+    T t[B];
+#pragma unroll
+    for (int n2 = 0; n2 < B; ++n2) t[n2] = v[n1 + A * n2];
+    dft<B, INV>(t);
+#pragma unroll
+    for (int k2 = 0; k2 < B; ++k2) u[n1 * B + k2] = twiddle_const<R, INV>(t[k2], n1 * k2);
+  }
+#pragma unroll
+  for (int k2 = 0; k2 < B; ++k2) {
+    T t[A];
+#pragma unroll
+    for (int n1 = 0; n1 < A; ++n1) t[n1] = u[n1 * B + k2];
+    dft<A, INV>(t);
+#pragma unroll
+    for (int k1 = 0; k1 < A; ++k1) v[k2 + B * k1] = t[k1];
+  }
+}
+
 template <int R, bool INV, typename T> __device__ __forceinline__ void dft(T* v) {
   if constexpr (R == 2) dft2<INV>(v);
   else if constexpr (R == 4) dft4<INV>(v);
   else if constexpr (R == 8) dft8<INV>(v);
-  else dft_odd<R, INV>(v);
-}
-
-// ---- one radix-R butterfly on shared memory ---------------------------------
-// DIF (forward):   v = x[q*stride]; v = DFT(v); v[q] *= w^(q*tws); store
-// DIT (inverse):   v = x[q*stride]; v[q] *= conj(w^(q*tws)); v = IDFT(v); store
-template <int R, typename T> __device__ __forceinline__ void bfly_dif(T* p, int stride, const T* tw, int tws) {
-  T v[R];
-#pragma unroll
-  for (int q = 0; q < R; ++q) v[q] = p[q * stride];
-  dft<R, false>(v);
-  if (tws) {
-#pragma unroll
-    for (int q = 1; q < R; ++q) v[q] = cmul(v[q], tw[q * tws]);
-  }
-#pragma unroll
-  for (int q = 0; q < R; ++q) p[q * stride] = v[q];
-}
-template <int R, typename T> __device__ __forceinline__ void bfly_dit(T* p, int stride, const T* tw, int tws) {
-  T v[R];
-#pragma unroll
-  for (int q = 0; q < R; ++q) v[q] = p[q * stride];
-  if (tws) {
-#pragma unroll
-    for (int q = 1; q < R; ++q) v[q] = cmulc(v[q], tw[q * tws]);
-  }
-  dft<R, true>(v);
-#pragma unroll
-  for (int q = 0; q < R; ++q) p[q * stride] = v[q];
-}
-
-template <int R, bool INV, typename T>
-__device__ __forceinline__ void bfly(T* p, int stride, const T* tw, int tws) {
-  if constexpr (INV) bfly_dit<R>(p, stride, tw, tws);
-  else bfly_dif<R>(p, stride, tw, tws);
+  else if constexpr (R == 3 || R == 5 || R == 7) dft_odd<R, INV>(v);
+  else if constexpr (R == 6) dft_ab<2, 3, INV>(v);
+  else if constexpr (R == 9) dft_ab<3, 3, INV>(v);
+  else if constexpr (R == 10) dft_ab<2, 5, INV>(v);
+  else if constexpr (R == 12) dft_ab<4, 3, INV>(v);
+  else if constexpr (R == 14) dft_ab<2, 7, INV>(v);
+  else if constexpr (R == 16) dft_ab<4, 4, INV>(v);
+  else static_assert(R == 2, "unsupported radix");
 }
 
 // Per-axis FFT description, passed by value to the kernels.
@@ -179,39 +245,5 @@ struct AxisFFT {
   int rad[kMaxStages];    // stage radices (DIF order)
   int blk[kMaxStages];    // sub-transform length entering each DIF stage
 };
-
-// Run all stages of a length-M transform on a [M][W] shared-memory tile.
-// Thread jobs are (butterfly, column) pairs with the column fastest, so a
-// quarter-warp touches contiguous 16-byte words (no bank conflicts).
-template <bool INV, int W, typename T>
-__device__ __forceinline__ void fft_stages(T* sm, const T* tw, const AxisFFT& ax) {
-  const int M = ax.M;
-  for (int si = 0; si < ax.nst; ++si) {
-    const int s = INV ? ax.nst - 1 - si : si;
-    const int r = ax.rad[s];
-    const int B = ax.blk[s];
-    const int span = B / r;
-    const int tstep = M / B;
-    const int njobs = (M / r) * W;
-    for (int job = threadIdx.x; job < njobs; job += blockDim.x) {
-      const int col = job % W;
-      const int t = job / W;
-      const int b = t / span;
-      const int j = t - b * span;
-      T* p = sm + (b * B + j) * W + col;
-      const int stride = span * W;
-      const int tws = j * tstep;
-      switch (r) {
-        case 2: bfly<2, INV>(p, stride, tw, tws); break;
-        case 3: bfly<3, INV>(p, stride, tw, tws); break;
-        case 4: bfly<4, INV>(p, stride, tw, tws); break;
-        case 5: bfly<5, INV>(p, stride, tw, tws); break;
-        case 7: bfly<7, INV>(p, stride, tw, tws); break;
-        default: bfly<8, INV>(p, stride, tw, tws); break;
-      }
-    }
-    __syncthreads();
-  }
-}
 
 }  // namespace bdda

@@ -14,221 +14,151 @@
 #include <cmath>
 #include <cstring>
 #include <type_traits>
+#include <algorithm>
+#include <vector>
 
 #include "bdda_internal.h"
 
+#include "bdda_pencil.cuh"
+
 namespace bdda {
 
-enum PassKind { K_FWD = 0, K_FWD_GATHER = 1, K_GREEN_Z = 2, K_CONV = 3, K_INV = 4, K_INV_SCATTER = 5 };
-
-struct PassArgs {
-  AxisFFT ax;
-  int n_in, n_out;      // rows read (the rest are zero) / rows written
-  int P1;               // pencil index p = p0 * P1 + p1
-  int ntile;            // column tiles per pencil
-  int L;                // right-hand sides
-  int64_t C;            // complex values per grid row (3L)
-  int64_t src_p0, src_p1, src_row;
-  int64_t dst_p0, dst_p1, dst_row;
-  const void* src;
-  void* dst;
-  const void* tw;       // this axis' twiddles, M entries
-  const int32_t* cell_map;
-  int64_t cell_p0, cell_p1;
-  const void* S;
-  const void* diag;
-  const void* jpre;
-  double scale;
-  const void* ghat;
-  int gN[3], gM[3];
-  double lf, k;
-};
-
-__device__ __forceinline__ bool axis_disp(int I, int N, int M, int& d) {
-  if (I <= N - 1) { d = I; return true; }
-  if (I >= M - (N - 1)) { d = I - M; return true; }
-  d = 0;
-  return false;
-}
-
-// Six unique components of A'(r) at cyclic index (ix, iy, iz)
-// (mvp_fft/mvp_fft.py:49-92 with the displacement map generalised to M >= 2N-1).
-__device__ void green_row(const PassArgs& a, int ix, int iy, int iz, double2* out) {
-  int dx, dy, dz;
-  const bool ok = axis_disp(ix, a.gN[0], a.gM[0], dx) & axis_disp(iy, a.gN[1], a.gM[1], dy) &
-                  axis_disp(iz, a.gN[2], a.gM[2], dz);
-  if (!ok || (dx == 0 && dy == 0 && dz == 0)) {
-    for (int c = 0; c < 6; ++c) out[c] = make_double2(0.0, 0.0);
-    return;
-  }
-  const double X = dx * a.lf, Y = dy * a.lf, Z = dz * a.lf;
-  const double r = sqrt(X * X + Y * Y + Z * Z);
-  const double u[3] = {X / r, Y / r, Z / r};
-  double sn, cs;
-  sincos(a.k * r, &sn, &cs);
-  const double pr = cs / r, pim = sn / r;            // e^{ikr} / r
-  const double nr = 1.0 / (r * r), ni = -a.k / r;    // (1 - ikr) / r^2
-  const double k2 = a.k * a.k;
-  const int ia[6] = {0, 0, 0, 1, 1, 2}, ib[6] = {0, 1, 2, 1, 2, 2};
-#pragma unroll
-  for (int c = 0; c < 6; ++c) {
-    const double uu = u[ia[c]] * u[ib[c]];
-    const double delta = (ia[c] == ib[c]) ? 1.0 : 0.0;
-    const double q = delta - 3.0 * uu;
-    const double tr = k2 * (uu - delta) + nr * q, ti = ni * q;
-    out[c] = make_double2(pr * tr - pim * ti, pr * ti + pim * tr);
-  }
-}
-
+// Generic pencil kernel: runtime radix sequence (any length factored into
+// radices <= RadixCap).  The specialised kernels (bdda_fixed_*.cu) replace it
+// for the radix sequences the workloads use.
 template <typename T, int KIND, int LT>
 __global__ void __launch_bounds__(256) pencil_kernel(const PassArgs a) {
-  constexpr int W = 3 * LT;
-  typedef typename real_of<T>::type F;
   extern __shared__ __align__(16) unsigned char smraw[];
-  const int M = a.ax.M;
-  T* tw = reinterpret_cast<T*>(smraw);
-  T* sm = tw + M;
-  const int tile = blockIdx.x % a.ntile;
-  const int64_t p = blockIdx.x / a.ntile;
-  const int64_t p0 = p / a.P1, p1 = p - p0 * a.P1;
-
-  const T* twg = static_cast<const T*>(a.tw);
-  for (int i = threadIdx.x; i < M; i += blockDim.x) tw[i] = twg[i];
-
-  // ---- load one pencil x tile into shared memory (zero beyond n_in) ----
-  if constexpr (KIND == K_GREEN_Z) {
+  const int M = a.ax.M, nst = a.ax.nst;
+  T *tw, *sm, *gs;
+  stage_constants<T, KIND, LT>(a, smraw, M, &tw, &sm, &gs);
+  const Pen c = pen_of_block(a);
+  if constexpr (KIND == K_FWD) {
+    bool staged = false;
     if constexpr (std::is_same<T, double2>::value) {
-      for (int i = threadIdx.x; i < M; i += blockDim.x) green_row(a, (int)p0, (int)p1, i, sm + i * W);
-    }
-  } else {
-    const T* src = static_cast<const T*>((KIND == K_FWD_GATHER && a.cell_map) ? a.S : a.src);
-    const int64_t base = p0 * a.src_p0 + p1 * a.src_p1;
-    const int total = M * W;
-    constexpr int U = 4;
-    for (int e0 = threadIdx.x; e0 < total; e0 += U * blockDim.x) {
-      T v[U];
-#pragma unroll
-      for (int u = 0; u < U; ++u) {
-        const int e = e0 + u * blockDim.x;
-        const int i = e / W, c = e - i * W;
-        const int comp = c / LT, l = tile * LT + (c - comp * LT);
-        v[u] = mkc<T>(F(0), F(0));
-        if (e < total && i < a.n_in && l < a.L) {
-          const int64_t gcol = (int64_t)comp * a.L + l;
-          if constexpr (KIND == K_FWD_GATHER) {
-            const int64_t cell = p0 * a.cell_p0 + p1 * a.cell_p1 + i;
-            if (a.cell_map) {
-              const int m = a.cell_map[cell];
-              if (m >= 0) v[u] = src[(int64_t)m * a.C + gcol];
-            } else {
-              v[u] = src[cell * a.C + gcol];
-            }
-          } else {
-            v[u] = src[base + (int64_t)i * a.src_row + gcol];
-          }
-        }
-      }
-#pragma unroll
-      for (int u = 0; u < U; ++u) {
-        const int e = e0 + u * blockDim.x;
-        if (e < total) sm[e] = v[u];
+      if (a.green) {   // real-space tensor rows evaluated into the tile (3 LT == 6)
+        for (int i = threadIdx.x; i < M; i += blockDim.x)
+          green_row(a, (int)c.p0, (int)c.p1, i, reinterpret_cast<double2*>(sm) + i * 3 * LT);
+        __syncthreads();
+        staged = true;
       }
     }
-  }
-  __syncthreads();
-
-  // ---- transform ----
-  if constexpr (KIND == K_INV || KIND == K_INV_SCATTER) {
-    fft_stages<true, W>(sm, tw, a.ax);
-  } else {
-    fft_stages<false, W>(sm, tw, a.ax);
-  }
-
-  if constexpr (KIND == K_CONV) {
-    // per-frequency y = G v with G complex symmetric: the 6 unique entries of
-    // this x-pencil are read once for all LT right-hand sides of the tile
-    const T* g = static_cast<const T*>(a.ghat) + p * (int64_t)M * 6;
-    for (int job = threadIdx.x; job < M * LT; job += blockDim.x) {
-      const int px = job / LT, li = job - px * LT;
-      T* r = sm + px * W + li;
-      const T v0 = r[0], v1 = r[LT], v2 = r[2 * LT];
-      const T* gp = g + px * 6;
-      const T gxx = gp[0], gxy = gp[1], gxz = gp[2], gyy = gp[3], gyz = gp[4], gzz = gp[5];
-      r[0] = cadd(cadd(cmul(gxx, v0), cmul(gxy, v1)), cmul(gxz, v2));
-      r[LT] = cadd(cadd(cmul(gxy, v0), cmul(gyy, v1)), cmul(gyz, v2));
-      r[2 * LT] = cadd(cadd(cmul(gxz, v0), cmul(gyz, v1)), cmul(gzz, v2));
+    if (nst == 1) {
+      if (staged) run_stage<false, 0, 1, KIND, T, LT>(a, c, sm, tw, 0);
+      else run_stage<false, 1, 1, KIND, T, LT>(a, c, sm, tw, 0);
+      return;
     }
+    if (staged) run_stage<false, 0, 0, KIND, T, LT>(a, c, sm, tw, 0);
+    else run_stage<false, 1, 0, KIND, T, LT>(a, c, sm, tw, 0);
     __syncthreads();
-    fft_stages<true, W>(sm, tw, a.ax);
-  }
-
-  // ---- store n_out rows ----
-  const int total = a.n_out * W;
-  for (int e = threadIdx.x; e < total; e += blockDim.x) {
-    const int i = e / W, c = e - i * W;
-    const int comp = c / LT, l = tile * LT + (c - comp * LT);
-    if (l >= a.L) continue;
-    const int64_t gcol = (int64_t)comp * a.L + l;
-    const T v = sm[e];
-    if constexpr (KIND == K_INV_SCATTER) {
-      const int64_t cell = p0 * a.cell_p0 + p1 * a.cell_p1 + i;
-      const F sc = F(a.scale);
-      T* out = static_cast<T*>(a.dst);
-      if (a.cell_map) {
-        const int m = a.cell_map[cell];
-        if (m >= 0) {
-          const int64_t row = 3 * (int64_t)m + comp;
-          const int64_t idx = (int64_t)m * a.C + gcol;
-          const T d = static_cast<const T*>(a.diag)[row];
-          const T j = static_cast<const T*>(a.jpre)[row];
-          const T s = static_cast<const T*>(a.S)[idx];
-          out[idx] = cmul(cadd(cmul(d, s), cscale(v, sc)), j);
-        }
-      } else {
-        out[cell * a.C + gcol] = cscale(v, sc);
-      }
-    } else {
-      static_cast<T*>(a.dst)[p0 * a.dst_p0 + p1 * a.dst_p1 + (int64_t)i * a.dst_row + gcol] = v;
+    for (int s = 1; s < nst - 1; ++s) {
+      run_stage<false, 0, 0, KIND, T, LT>(a, c, sm, tw, s);
+      __syncthreads();
     }
+    run_stage<false, 0, 1, KIND, T, LT>(a, c, sm, tw, nst - 1);
+  } else if constexpr (KIND == K_INV) {
+    if (nst == 1) {
+      run_stage<true, 1, 1, KIND, T, LT>(a, c, sm, tw, 0);
+      return;
+    }
+    run_stage<true, 1, 0, KIND, T, LT>(a, c, sm, tw, nst - 1);
+    __syncthreads();
+    for (int s = nst - 2; s >= 1; --s) {
+      run_stage<true, 0, 0, KIND, T, LT>(a, c, sm, tw, s);
+      __syncthreads();
+    }
+    run_stage<true, 0, 1, KIND, T, LT>(a, c, sm, tw, 0);
+  } else {   // K_CONV
+    cp_async_wait<0>();
+    __syncthreads();
+    if (nst == 1) {
+      run_conv_mid<1, 1, T, LT>(a, c, sm, gs);
+      return;
+    }
+    run_stage<false, 1, 0, KIND, T, LT>(a, c, sm, tw, 0);
+    __syncthreads();
+    for (int s = 1; s < nst - 1; ++s) {
+      run_stage<false, 0, 0, KIND, T, LT>(a, c, sm, tw, s);
+      __syncthreads();
+    }
+    run_conv_mid<0, 0, T, LT>(a, c, sm, gs);
+    __syncthreads();
+    for (int s = nst - 2; s >= 1; --s) {
+      run_stage<true, 0, 0, KIND, T, LT>(a, c, sm, tw, s);
+      __syncthreads();
+    }
+    run_stage<true, 0, 1, KIND, T, LT>(a, c, sm, tw, 0);
   }
 }
 
-// Shared-memory budget per CTA for the pencil tiles; tiles are chosen as wide
-// as fit (at most 3 CTAs per SM at the default).
-static size_t g_tile_smem_budget = 72 * 1024;
+template <typename T>
+static size_t pencil_smem(int M, int LT, int kind) {
+  return (size_t)pencil_smem_bytes<T>(M, LT, kind);
+}
 
-static int pick_lt(int M, int L, size_t esz) {
-  const int cand[4] = {8, 4, 2, 1};
+// Launch shape of the pencil passes, per precision (0 c128, 1 c64) and pass
+// kind: the shared-memory budget per CTA (the widest column tile that fits is
+// used) and the threads per CTA.  Set by bdda_tune_set.
+static size_t g_tile_smem_budget[2][3] = {{72 * 1024, 72 * 1024, 72 * 1024},
+                                          {72 * 1024, 72 * 1024, 72 * 1024}};
+static int g_threads[2][3] = {{256, 256, 256}, {256, 256, 256}};
+static_assert(K_FWD == 0 && K_CONV == 1 && K_INV == 2, "tuning tables are indexed by pass kind");
+
+template <typename T>
+static int pick_lt(int M, int L, int kind) {
+  const int cand[3] = {8, 4, 2};
   for (int lt : cand) {
-    if (lt > 1 && lt / 2 >= L) continue;
-    if ((size_t)M * (1 + 3 * lt) * esz <= g_tile_smem_budget) return lt;
+    if (lt > 2 && lt / 2 >= L) continue;
+    if (pencil_smem<T>(M, lt, kind) <= g_tile_smem_budget[prec_of<T>()][kind]) return lt;
   }
-  return 1;
+  return 2;
 }
 
 template <typename T, int KIND, int LT>
 static int launch_lt(PassArgs a, int64_t P0, cudaStream_t st) {
   auto kern = pencil_kernel<T, KIND, LT>;
   a.ntile = (a.L + LT - 1) / LT;
-  const size_t smem = (size_t)a.ax.M * (1 + 3 * LT) * sizeof(T);
+  const size_t smem = pencil_smem<T>(a.ax.M, LT, KIND);
   if (smem > 227 * 1024) return BDDA_BAD_ARG;
   const int64_t nblk = P0 * a.P1 * a.ntile;
   if (nblk <= 0) return BDDA_OK;
   if (nblk > INT_MAX) return BDDA_BAD_ARG;
   BDDA_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  kern<<<(unsigned)nblk, 256, smem, st>>>(a);
+  kern<<<(unsigned)nblk, g_threads[prec_of<T>()][KIND], smem, st>>>(a);
   BDDA_CUDA_TRY(cudaGetLastError());
   count_launch();
   return BDDA_OK;
 }
 
+static int g_use_fixed = 1;   // specialised kernels on (bdda_tune_fixed)
+
+static FixedLaunchFn fixed_find(int prec, int kind, int lt, const AxisFFT& ax) {
+  if (!g_use_fixed || ax.nst > 4) return nullptr;
+  int r[4] = {1, 1, 1, 1};
+  for (int s = 0; s < ax.nst; ++s) r[s] = ax.rad[s];
+  for (int t = 0; t < 2; ++t) {
+    int n = 0;
+    const FixedKernel* tab = t == 0 ? fixed_table_a(&n) : fixed_table_b(&n);
+    for (int i = 0; i < n; ++i) {
+      const FixedKernel& f = tab[i];
+      if (f.prec == prec && f.kind == kind && f.lt == lt && f.r[0] == r[0] && f.r[1] == r[1] &&
+          f.r[2] == r[2] && f.r[3] == r[3])
+        return f.fn;
+    }
+  }
+  return nullptr;
+}
+
 template <typename T, int KIND>
 static int launch_pass(const PassArgs& a, int64_t P0, int lt, cudaStream_t st) {
+  if (!a.green) {
+    FixedLaunchFn f = fixed_find(prec_of<T>(), KIND, lt, a.ax);
+    if (f) return f(a, P0, st);
+  }
   switch (lt) {
     case 8: return launch_lt<T, KIND, 8>(a, P0, st);
     case 4: return launch_lt<T, KIND, 4>(a, P0, st);
-    case 2: return launch_lt<T, KIND, 2>(a, P0, st);
-    default: return launch_lt<T, KIND, 1>(a, P0, st);
+    default: return launch_lt<T, KIND, 2>(a, P0, st);
   }
 }
 
@@ -254,6 +184,7 @@ static int run_mvp(const bdda_plan* plan, int L, const T* ghat, const int32_t* c
   memset(&b, 0, sizeof(b));
   b.L = L;
   b.C = C;
+  b.scale = 1.0;
   const bool prof = profiling();
   if (prof) profile_mark(0, st);
 
@@ -262,20 +193,20 @@ static int run_mvp(const bdda_plan* plan, int L, const T* ghat, const int32_t* c
     a.ax = plan->ax[2]; a.tw = table_ptr<T>(plan, TwOff<T>::get(plan, 2));
     a.n_in = (int)Nz; a.n_out = (int)Mz; a.P1 = (int)Ny;
     a.cell_map = cell_map; a.cell_p0 = Ny * Nz; a.cell_p1 = Nz;
-    a.S = src; a.src = src;
+    a.S = src;
+    a.src = src; a.src_p0 = Ny * Nz * C; a.src_p1 = Nz * C; a.src_row = C;   // dense cuboid input
     a.dst = F; a.dst_p0 = My * Mz * C; a.dst_p1 = Mz * C; a.dst_row = C;
-    BDDA_TRY((launch_pass<T, K_FWD_GATHER>(a, Nx, pick_lt((int)Mz, L, sizeof(T)), st)));
+    BDDA_TRY((launch_pass<T, K_FWD>(a, Nx, pick_lt<T>((int)Mz, L, K_FWD), st)));
     if (prof) profile_mark(1, st);
   }
   PassArgs ay = b;  // Y and Y^-1 share the pencil geometry
   ay.ax = plan->ax[1]; ay.tw = table_ptr<T>(plan, TwOff<T>::get(plan, 1));
   ay.P1 = (int)Mz; ay.src = F; ay.dst = F;
   ay.src_p0 = ay.dst_p0 = My * Mz * C; ay.src_p1 = ay.dst_p1 = C; ay.src_row = ay.dst_row = Mz * C;
-  const int lty = pick_lt((int)My, L, sizeof(T));
   {
     PassArgs a = ay;
     a.n_in = (int)Ny; a.n_out = (int)My;
-    BDDA_TRY((launch_pass<T, K_FWD>(a, Nx, lty, st)));
+    BDDA_TRY((launch_pass<T, K_FWD>(a, Nx, pick_lt<T>((int)My, L, K_FWD), st)));
     if (prof) profile_mark(2, st);
   }
   {  // X: forward, Green multiply, inverse
@@ -285,13 +216,13 @@ static int run_mvp(const bdda_plan* plan, int L, const T* ghat, const int32_t* c
     a.src = F; a.dst = F;
     a.src_p0 = a.dst_p0 = Mz * C; a.src_p1 = a.dst_p1 = C; a.src_row = a.dst_row = My * Mz * C;
     a.ghat = ghat;
-    BDDA_TRY((launch_pass<T, K_CONV>(a, My, pick_lt((int)Mx, L, sizeof(T)), st)));
+    BDDA_TRY((launch_pass<T, K_CONV>(a, My, pick_lt<T>((int)Mx, L, K_CONV), st)));
     if (prof) profile_mark(3, st);
   }
   {
     PassArgs a = ay;
     a.n_in = (int)My; a.n_out = (int)Ny;
-    BDDA_TRY((launch_pass<T, K_INV>(a, Nx, lty, st)));
+    BDDA_TRY((launch_pass<T, K_INV>(a, Nx, pick_lt<T>((int)My, L, K_INV), st)));
     if (prof) profile_mark(4, st);
   }
   {  // Z^-1 + crop + epilogue
@@ -300,9 +231,10 @@ static int run_mvp(const bdda_plan* plan, int L, const T* ghat, const int32_t* c
     a.n_in = (int)Mz; a.n_out = (int)Nz; a.P1 = (int)Ny;
     a.src = F; a.src_p0 = My * Mz * C; a.src_p1 = Mz * C; a.src_row = C;
     a.cell_map = cell_map; a.cell_p0 = Ny * Nz; a.cell_p1 = Nz;
-    a.S = src; a.diag = diag; a.jpre = jpre; a.dst = out;
+    a.S = src; a.diag = diag; a.jpre = jpre;
+    a.dst = out; a.dst_p0 = Ny * Nz * C; a.dst_p1 = Nz * C; a.dst_row = C;   // dense cuboid output
     a.scale = 1.0 / (double)(Mx * My * Mz);
-    BDDA_TRY((launch_pass<T, K_INV_SCATTER>(a, Nx, pick_lt((int)Mz, L, sizeof(T)), st)));
+    BDDA_TRY((launch_pass<T, K_INV>(a, Nx, pick_lt<T>((int)Mz, L, K_INV), st)));
     if (prof) profile_mark(5, st);
   }
   return BDDA_OK;
@@ -388,21 +320,75 @@ static bool smooth7(int m) {
   return m == 1;
 }
 
-static int factor_axis(int M, AxisFFT& ax) {
-  int m = M, ns = 0;
-  int r[kMaxStages];
-  while (m % 8 == 0 && ns < kMaxStages) { r[ns++] = 8; m /= 8; }
-  if (m % 4 == 0 && ns < kMaxStages) { r[ns++] = 4; m /= 4; }
-  if (m % 2 == 0 && ns < kMaxStages) { r[ns++] = 2; m /= 2; }
-  for (int p : {3, 5, 7})
-    while (m % p == 0 && ns < kMaxStages) { r[ns++] = p; m /= p; }
-  if (m != 1) return BDDA_BAD_ARG;
+// Radices with register kernels, largest first, and the caps the kernels
+// are compiled with (RadixCap): any stage <= kStageCap, the X-pass axis'
+// last stage (fused with the Green multiply) <= kMidCap.
+static const int kRadices[] = {16, 14, 12, 10, 9, 8, 7, 6, 5, 4, 3, 2};
+static const int kStageCap = 10;
+static const int kMidCap = 4;
+
+static void enum_factorizations(int m, int maxr, std::vector<int>& cur, std::vector<std::vector<int>>& out) {
+  if (m == 1) { out.push_back(cur); return; }
+  if ((int)cur.size() >= 6) return;
+  for (int r : kRadices)
+    if (r <= maxr && m % r == 0) {
+      cur.push_back(r);
+      enum_factorizations(m / r, r, cur, out);
+      cur.pop_back();
+    }
+}
+
+// Fewest stages first, then the most balanced sequence (smallest largest
+// radix); radices run largest first.  The X-pass axis (conv) keeps its last
+// radix <= kMidCap so the fused middle (3 components x R frequencies on
+// registers) stays small.  Returns the stage count (0: no factorization).
+static int best_factorization(int M, bool conv, std::vector<int>& best) {
+  std::vector<std::vector<int>> all;
+  std::vector<int> cur;
+  enum_factorizations(M, kStageCap, cur, all);
+  int best_key = INT_MAX;
+  best.clear();
+  for (const auto& f : all) {
+    if (conv && f.back() > kMidCap) continue;
+    const int key = (int)f.size() * 64 + f.front();
+    if (key < best_key) { best_key = key; best = f; }
+  }
+  return (int)best.size();
+}
+
+static int factor_axis(int M, bool conv, AxisFFT& ax) {
+  std::vector<int> r;
+  if (M == 1) {
+    r.clear();
+  } else if (best_factorization(M, conv, r) == 0 || (int)r.size() > kMaxStages) {
+    return BDDA_BAD_ARG;
+  }
   ax.M = M;
-  ax.nst = ns;
+  ax.nst = (int)r.size();
   int B = M;
-  for (int s = 0; s < ns; ++s) { ax.rad[s] = r[s]; ax.blk[s] = B; B /= r[s]; }
-  for (int s = ns; s < kMaxStages; ++s) { ax.rad[s] = 1; ax.blk[s] = 1; }
+  for (int s = 0; s < ax.nst; ++s) { ax.rad[s] = r[s]; ax.blk[s] = B; B /= r[s]; }
+  for (int s = ax.nst; s < kMaxStages; ++s) { ax.rad[s] = 1; ax.blk[s] = 1; }
   return BDDA_OK;
+}
+
+// Cyclic length for a cuboid side N: the even 7-smooth M >= 2N minimising
+// M x (1 + 1/4 per radix stage beyond the first), searched up to 2N + 2N/4.
+static int choose_length(int N, bool conv) {
+  int best = -1;
+  double best_cost = 1e300;
+  for (int M = 2 * N; M <= 2 * N + (2 * N) / 4 + 2; M += 2) {
+    if (!smooth7(M)) continue;
+    std::vector<int> f;
+    const int ns = best_factorization(M, conv, f);
+    if (ns == 0) continue;
+    const double cost = M * (1.0 + 0.25 * (ns - 1));
+    if (cost < best_cost) { best_cost = cost; best = M; }
+  }
+  if (best < 0) {
+    best = 2 * N;
+    while (!smooth7(best)) best += 2;
+  }
+  return best;
 }
 
 }  // namespace bdda
@@ -428,6 +414,27 @@ const char* bdda_status_string(int s) {
 
 int bdda_version(void) { return 100; }
 
+int bdda_tune_set(int prec, int kind, size_t smem_budget, int threads) {
+  if (prec < 0 || prec > 1 || kind < 0 || kind > 2 || threads < 32 || threads > 512 || (threads & 31) ||
+      smem_budget < 1024 || smem_budget > 227 * 1024)
+    return BDDA_BAD_ARG;
+  g_tile_smem_budget[prec][kind] = smem_budget;
+  g_threads[prec][kind] = threads;
+  return BDDA_OK;
+}
+
+int bdda_tune_fixed(int on) {
+  g_use_fixed = on ? 1 : 0;
+  return BDDA_OK;
+}
+
+int bdda_tune_get(int prec, int kind, size_t* smem_budget, int* threads) {
+  if (prec < 0 || prec > 1 || kind < 0 || kind > 2 || !smem_budget || !threads) return BDDA_BAD_ARG;
+  *smem_budget = g_tile_smem_budget[prec][kind];
+  *threads = g_threads[prec][kind];
+  return BDDA_OK;
+}
+
 int bdda_plan_create(const int n[3], const int m[3], bdda_plan** out) {
   if (!n || !out) return BDDA_BAD_ARG;
   bdda_plan* p = new bdda_plan();
@@ -438,12 +445,11 @@ int bdda_plan_create(const int n[3], const int m[3], bdda_plan** out) {
     int M;
     if (m) {
       M = m[a];
-      if (M < 2 * n[a] - 1 || !smooth7(M)) { delete p; return BDDA_BAD_ARG; }
+      if (M < 2 * n[a] - 1 || M < 1 || !smooth7(M)) { delete p; return BDDA_BAD_ARG; }
     } else {
-      M = 2 * n[a];
-      while (!smooth7(M)) M += 2;
+      M = choose_length(n[a], a == 0);
     }
-    if (factor_axis(M, p->ax[a]) != BDDA_OK) { delete p; return BDDA_BAD_ARG; }
+    if (factor_axis(M, a == 0, p->ax[a]) != BDDA_OK) { delete p; return BDDA_BAD_ARG; }
   }
   // device tables: twiddles (both precisions) and position -> frequency maps
   size_t off = 0;
@@ -502,7 +508,7 @@ int bdda_plan_radices(const bdda_plan* p, int axis, int radices[12], int* nstage
 size_t bdda_plan_table_bytes(const bdda_plan* p) { return p ? p->table_bytes : 0; }
 
 int bdda_plan_attach_tables(bdda_plan* p, void* dev, void* stream) {
-  if (!p || !dev) return BDDA_BAD_ARG;
+  if (!p || !dev || (reinterpret_cast<uintptr_t>(dev) & 15)) return BDDA_BAD_ARG;
   BDDA_CUDA_TRY(cudaMemcpyAsync(dev, p->host_tables.data(), p->table_bytes, cudaMemcpyHostToDevice,
                                 (cudaStream_t)stream));
   // the host copy must not change before the upload completes
@@ -533,12 +539,14 @@ int bdda_green_build(const bdda_plan* p, double lf, double k, void* ghat, void* 
   for (int a = 0; a < 3; ++a) { b.gN[a] = p->n[a]; b.gM[a] = p->ax[a].M; }
   b.lf = lf;
   b.k = k;
-  {  // real-space tensor evaluated on the fly, forward z
+  b.scale = 1.0;
+  {  // real-space tensor evaluated in the kernel, forward z
     PassArgs a = b;
     a.ax = p->ax[2]; a.tw = table_ptr<double2>(p, p->tw64_off[2]);
     a.n_in = a.n_out = (int)Mz; a.P1 = (int)My;
+    a.green = 1;
     a.dst = G; a.dst_p0 = My * Mz * 6; a.dst_p1 = Mz * 6; a.dst_row = 6;
-    BDDA_TRY((launch_lt<double2, K_GREEN_Z, 2>(a, Mx, st)));
+    BDDA_TRY((launch_lt<double2, K_FWD, 2>(a, Mx, st)));
   }
   {  // forward y
     PassArgs a = b;
@@ -631,6 +639,7 @@ int bdda_occupancy_map(const bdda_plan* p, const int64_t* address, int n_occ, in
 int bdda_fft_mvp(const bdda_plan* p, int prec, int L, const void* ghat, const void* P_full,
                  void* Y_full, void* work, void* stream) {
   if (!p || L < 1 || !ghat || !P_full || !Y_full) return BDDA_BAD_ARG;
+  if (reinterpret_cast<uintptr_t>(ghat) & 15) return BDDA_BAD_ARG;   // staged with 16-byte async copies
   if (!work || !p->dev_tables) return BDDA_NO_WORKSPACE;
   cudaStream_t st = (cudaStream_t)stream;
   if (prec == BDDA_C128)
@@ -648,6 +657,7 @@ int bdda_block_mvp(const bdda_plan* p, int prec, int L, const void* ghat, const 
                    const void* diag, const void* jpre, const void* S, void* out, void* work,
                    void* stream) {
   if (!p || L < 1 || !ghat || !cell_map || !diag || !jpre || !S || !out) return BDDA_BAD_ARG;
+  if (reinterpret_cast<uintptr_t>(ghat) & 15) return BDDA_BAD_ARG;   // staged with 16-byte async copies
   if (!work || !p->dev_tables) return BDDA_NO_WORKSPACE;
   cudaStream_t st = (cudaStream_t)stream;
   if (prec == BDDA_C128)

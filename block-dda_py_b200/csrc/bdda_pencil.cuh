@@ -1,0 +1,329 @@
+// Device code shared by the pencil-pass kernels: pass arguments, global row
+// access of one pencil x column tile, radix-stage jobs, and the fused X-pass
+// middle (last forward stage, Green multiply, first inverse stage).
+//
+// A CTA owns one pencil (a line of the grid along the transformed axis) and a
+// column tile of LT right-hand sides x 3 components, staged in shared memory
+// as [row][3 LT].  The first radix stage reads global memory directly and the
+// last one writes it, so only the stages between round-trip through shared
+// memory.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <type_traits>
+
+#include "bdda_internal.h"
+
+namespace bdda {
+
+enum PassKind { K_FWD = 0, K_CONV = 1, K_INV = 2 };
+
+struct PassArgs {
+  AxisFFT ax;
+  int n_in, n_out;      // rows read (the rest are zero) / rows written
+  int P1;               // pencil index p = p0 * P1 + p1
+  int ntile;            // column tiles per pencil
+  int L;                // right-hand sides
+  int green;            // K_FWD: the rows are A'(r), evaluated in the kernel
+  int64_t C;            // complex values per grid row (3L)
+  int64_t src_p0, src_p1, src_row;
+  int64_t dst_p0, dst_p1, dst_row;
+  const void* src;
+  void* dst;
+  const void* tw;       // this axis' twiddles, M entries
+  const int32_t* cell_map;   // K_FWD: gather S through it; K_INV: scatter with the epilogue
+  int64_t cell_p0, cell_p1;
+  const void* S;
+  const void* diag;
+  const void* jpre;
+  double scale;         // K_INV: factor applied to the output (1/(Mx My Mz) in the last pass)
+  const void* ghat;
+  int gN[3], gM[3];
+  double lf, k;
+};
+
+struct Pen {
+  int64_t p0, p1;
+  int tile;
+};
+
+__device__ __forceinline__ bool axis_disp(int I, int N, int M, int& d) {
+  if (I <= N - 1) { d = I; return true; }
+  if (I >= M - (N - 1)) { d = I - M; return true; }
+  d = 0;
+  return false;
+}
+
+// Six unique components of A'(r) at cyclic index (ix, iy, iz)
+// (mvp_fft/mvp_fft.py:49-92 with the displacement map generalised to M >= 2N-1).
+static __device__ void green_row(const PassArgs& a, int ix, int iy, int iz, double2* out) {
+  int dx, dy, dz;
+  const bool ok = axis_disp(ix, a.gN[0], a.gM[0], dx) & axis_disp(iy, a.gN[1], a.gM[1], dy) &
+                  axis_disp(iz, a.gN[2], a.gM[2], dz);
+  if (!ok || (dx == 0 && dy == 0 && dz == 0)) {
+    for (int c = 0; c < 6; ++c) out[c] = make_double2(0.0, 0.0);
+    return;
+  }
+  const double X = dx * a.lf, Y = dy * a.lf, Z = dz * a.lf;
+  const double r = sqrt(X * X + Y * Y + Z * Z);
+  const double u[3] = {X / r, Y / r, Z / r};
+  double sn, cs;
+  sincos(a.k * r, &sn, &cs);
+  const double pr = cs / r, pim = sn / r;            // e^{ikr} / r
+  const double nr = 1.0 / (r * r), ni = -a.k / r;    // (1 - ikr) / r^2
+  const double k2 = a.k * a.k;
+  const int ia[6] = {0, 0, 0, 1, 1, 2}, ib[6] = {0, 1, 2, 1, 2, 2};
+#pragma unroll
+  for (int c = 0; c < 6; ++c) {
+    const double uu = u[ia[c]] * u[ib[c]];
+    const double delta = (ia[c] == ib[c]) ? 1.0 : 0.0;
+    const double q = delta - 3.0 * uu;
+    const double tr = k2 * (uu - delta) + nr * q, ti = ni * q;
+    out[c] = make_double2(pr * tr - pim * ti, pr * ti + pim * tr);
+  }
+}
+
+// ---- asynchronous global -> shared copies (cp.async, 16-byte granules) ----
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// nbytes is a multiple of 8; both pointers are 16-byte aligned
+__device__ __forceinline__ void async_copy(void* dst, const void* src, int nbytes) {
+  const int n16 = nbytes >> 4;
+  for (int i = threadIdx.x; i < n16; i += blockDim.x)
+    cp_async16(static_cast<char*>(dst) + 16 * i, static_cast<const char*>(src) + 16 * i);
+  if ((nbytes & 15) && threadIdx.x == 0)
+    *reinterpret_cast<uint2*>(static_cast<char*>(dst) + 16 * n16) =
+        *reinterpret_cast<const uint2*>(static_cast<const char*>(src) + 16 * n16);
+}
+
+__host__ __device__ __forceinline__ int align16(int x) { return (x + 15) & ~15; }
+
+template <typename T> constexpr int prec_of() { return std::is_same<T, double2>::value ? 0 : 1; }
+
+template <typename T>
+__host__ __device__ __forceinline__ int pencil_smem_bytes(int M, int LT, int kind) {
+  return align16(M * (int)sizeof(T)) + align16(M * 3 * LT * (int)sizeof(T)) +
+         (kind == K_CONV ? align16(M * 6 * (int)sizeof(T)) : 0);
+}
+
+// Pencil and tile of a CTA (one item per CTA).
+__device__ __forceinline__ Pen pen_of_block(const PassArgs& a) {
+  Pen c;
+  c.tile = (int)(blockIdx.x % a.ntile);
+  const int64_t p = blockIdx.x / a.ntile;
+  c.p0 = p / a.P1;
+  c.p1 = p - c.p0 * a.P1;
+  return c;
+}
+
+// Shared-memory carve-up and the asynchronous staging of the twiddles (and,
+// for the X pass, the Green's pencil).  Returns after the twiddles landed.
+template <typename T, int KIND, int LT>
+__device__ __forceinline__ void stage_constants(const PassArgs& a, unsigned char* smraw, int M, T** tw, T** sm,
+                                                T** gs) {
+  *tw = reinterpret_cast<T*>(smraw);
+  *sm = reinterpret_cast<T*>(smraw + align16(M * (int)sizeof(T)));
+  *gs = reinterpret_cast<T*>(smraw + align16(M * (int)sizeof(T)) + align16(M * 3 * LT * (int)sizeof(T)));
+  async_copy(*tw, a.tw, M * (int)sizeof(T));
+  cp_async_commit();
+  if constexpr (KIND == K_CONV) {
+    const int64_t p = blockIdx.x / a.ntile;
+    async_copy(*gs, static_cast<const T*>(a.ghat) + p * (int64_t)M * 6, M * 6 * (int)sizeof(T));
+  }
+  cp_async_commit();
+  cp_async_wait<1>();
+  __syncthreads();
+}
+
+
+
+// ---- global row access of one pencil x column tile ----
+template <int KIND, typename T, int LT>
+__device__ __forceinline__ T gload(const PassArgs& a, const Pen& c, int row, int col) {
+  typedef typename real_of<T>::type F;
+  const int comp = col / LT, l = c.tile * LT + (col - comp * LT);
+  if (row >= a.n_in || l >= a.L) return mkc<T>(F(0), F(0));
+  const int64_t gcol = (int64_t)comp * a.L + l;
+  if constexpr (KIND == K_FWD) {
+    if (a.cell_map) {
+      const int m = a.cell_map[c.p0 * a.cell_p0 + c.p1 * a.cell_p1 + row];
+      return m >= 0 ? static_cast<const T*>(a.S)[(int64_t)m * a.C + gcol] : mkc<T>(F(0), F(0));
+    }
+  }
+  return static_cast<const T*>(a.src)[c.p0 * a.src_p0 + c.p1 * a.src_p1 + (int64_t)row * a.src_row + gcol];
+}
+
+template <int KIND, typename T, int LT>
+__device__ __forceinline__ void gstore(const PassArgs& a, const Pen& c, int row, int col, T v) {
+  typedef typename real_of<T>::type F;
+  const int comp = col / LT, l = c.tile * LT + (col - comp * LT);
+  if (row >= a.n_out || l >= a.L) return;
+  const int64_t gcol = (int64_t)comp * a.L + l;
+  if constexpr (KIND == K_INV) {
+    const F sc = F(a.scale);
+    if (a.cell_map) {   // crop + gather + diagonal + Jacobi: (diag S + y) jpre (bl_krylov.py:55)
+      const int m = a.cell_map[c.p0 * a.cell_p0 + c.p1 * a.cell_p1 + row];
+      if (m >= 0) {
+        const int64_t r3 = 3 * (int64_t)m + comp;
+        const int64_t idx = (int64_t)m * a.C + gcol;
+        const T d = static_cast<const T*>(a.diag)[r3];
+        const T j = static_cast<const T*>(a.jpre)[r3];
+        const T s = static_cast<const T*>(a.S)[idx];
+        static_cast<T*>(a.dst)[idx] = cmul(cadd(cmul(d, s), cscale(v, sc)), j);
+      }
+      return;
+    }
+    v = cscale(v, sc);
+  }
+  static_cast<T*>(a.dst)[c.p0 * a.dst_p0 + c.p1 * a.dst_p1 + (int64_t)row * a.dst_row + gcol] = v;
+}
+
+// ---- one radix-R butterfly of a stage; rows base + q*span of column col ----
+// forward (DIF): DFT then twiddles w^(q*tws); inverse (DIT): conj twiddles then IDFT.
+// SRC / DST: 1 = global (fused with the load or the store), 0 = shared.
+template <int R, bool INV, int SRC, int DST, int KIND, typename T, int LT>
+__device__ __forceinline__ void stage_job(const PassArgs& a, const Pen& c, T* sm, const T* tw, int col,
+                                          int base, int span, int tws) {
+  constexpr int W = 3 * LT;
+  T v[R];
+#pragma unroll
+  for (int q = 0; q < R; ++q) {
+    const int row = base + q * span;
+    if constexpr (SRC) v[q] = gload<KIND, T, LT>(a, c, row, col);
+    else v[q] = sm[row * W + col];
+  }
+  if constexpr (!INV) {
+    dft<R, false>(v);
+    if (tws) {
+#pragma unroll
+      for (int q = 1; q < R; ++q) v[q] = cmul(v[q], tw[q * tws]);
+    }
+  } else {
+    if (tws) {
+#pragma unroll
+      for (int q = 1; q < R; ++q) v[q] = cmulc(v[q], tw[q * tws]);
+    }
+    dft<R, true>(v);
+  }
+#pragma unroll
+  for (int q = 0; q < R; ++q) {
+    const int row = base + q * span;
+    if constexpr (DST) gstore<KIND, T, LT>(a, c, row, col, v[q]);
+    else sm[row * W + col] = v[q];
+  }
+}
+
+// Largest radix compiled into the kernels of one element type (register
+// budget: R complex values per job, 3 R in the X-pass middle).
+template <typename T> struct RadixCap;
+template <> struct RadixCap<double2> { static constexpr int stage = 10, mid = 4; };
+template <> struct RadixCap<float2> { static constexpr int stage = 10, mid = 4; };
+
+template <bool INV, int SRC, int DST, int KIND, typename T, int LT>
+__device__ void run_stage(const PassArgs& a, const Pen& c, T* sm, const T* tw, int s) {
+  constexpr int W = 3 * LT;
+  const int M = a.ax.M, r = a.ax.rad[s], B = a.ax.blk[s];
+  const int span = B / r, tstep = M / B;
+  const int njobs = (M / r) * W;
+  for (int job = threadIdx.x; job < njobs; job += blockDim.x) {
+    const int col = job % W;
+    const int t = job / W;
+    const int b = t / span;
+    const int j = t - b * span;
+    const int base = b * B + j, tws = j * tstep;
+    switch (r) {
+#define BDDA_RADIX_CASE(RR)                                                          \
+  case RR:                                                                           \
+    if constexpr (RR <= RadixCap<T>::stage)                                          \
+      stage_job<RR, INV, SRC, DST, KIND, T, LT>(a, c, sm, tw, col, base, span, tws); \
+    break;
+      BDDA_RADIX_CASE(2) BDDA_RADIX_CASE(3) BDDA_RADIX_CASE(4) BDDA_RADIX_CASE(5) BDDA_RADIX_CASE(6)
+      BDDA_RADIX_CASE(7) BDDA_RADIX_CASE(8) BDDA_RADIX_CASE(9) BDDA_RADIX_CASE(10) BDDA_RADIX_CASE(12)
+      BDDA_RADIX_CASE(14) BDDA_RADIX_CASE(16)
+#undef BDDA_RADIX_CASE
+      default: break;
+    }
+  }
+}
+
+// X pass middle: the last forward stage (span 1), the per-frequency 3x3
+// complex-symmetric Green multiply and the first inverse stage (span 1) on
+// registers; one job = R consecutive frequencies x all 3 components of one
+// right-hand side, so the 6 unique entries are read once per frequency and
+// right-hand side from the pencil staged in shared memory.
+template <int R, int SRC, int DST, typename T, int LT>
+__device__ __forceinline__ void conv_mid_job(const PassArgs& a, const Pen& c, T* sm, const T* gs, int b,
+                                             int li) {
+  constexpr int W = 3 * LT;
+  T y[3][R];
+#pragma unroll
+  for (int comp = 0; comp < 3; ++comp) {
+#pragma unroll
+    for (int q = 0; q < R; ++q) {
+      const int row = b * R + q, col = comp * LT + li;
+      if constexpr (SRC) y[comp][q] = gload<K_CONV, T, LT>(a, c, row, col);
+      else y[comp][q] = sm[row * W + col];
+    }
+    dft<R, false>(y[comp]);
+  }
+#pragma unroll
+  for (int q = 0; q < R; ++q) {
+    const T* g = gs + (b * R + q) * 6;
+    const T gxx = g[0], gxy = g[1], gxz = g[2], gyy = g[3], gyz = g[4], gzz = g[5];
+    const T v0 = y[0][q], v1 = y[1][q], v2 = y[2][q];
+    y[0][q] = cadd(cadd(cmul(gxx, v0), cmul(gxy, v1)), cmul(gxz, v2));
+    y[1][q] = cadd(cadd(cmul(gxy, v0), cmul(gyy, v1)), cmul(gyz, v2));
+    y[2][q] = cadd(cadd(cmul(gxz, v0), cmul(gyz, v1)), cmul(gzz, v2));
+  }
+#pragma unroll
+  for (int comp = 0; comp < 3; ++comp) {
+    dft<R, true>(y[comp]);
+#pragma unroll
+    for (int q = 0; q < R; ++q) {
+      const int row = b * R + q, col = comp * LT + li;
+      if constexpr (DST) gstore<K_CONV, T, LT>(a, c, row, col, y[comp][q]);
+      else sm[row * W + col] = y[comp][q];
+    }
+  }
+}
+
+template <int SRC, int DST, typename T, int LT>
+__device__ void run_conv_mid(const PassArgs& a, const Pen& c, T* sm, const T* gs) {
+  const int r = a.ax.rad[a.ax.nst - 1];
+  const int njobs = (a.ax.M / r) * LT;
+  for (int job = threadIdx.x; job < njobs; job += blockDim.x) {
+    const int li = job % LT, b = job / LT;
+    switch (r) {
+#define BDDA_MID_CASE(RR)                                        \
+  case RR:                                                         \
+    if constexpr (RR <= RadixCap<T>::mid)                          \
+      conv_mid_job<RR, SRC, DST, T, LT>(a, c, sm, gs, b, li);      \
+    break;
+      BDDA_MID_CASE(2) BDDA_MID_CASE(3) BDDA_MID_CASE(4) BDDA_MID_CASE(5) BDDA_MID_CASE(6)
+      BDDA_MID_CASE(7) BDDA_MID_CASE(8) BDDA_MID_CASE(9) BDDA_MID_CASE(10) BDDA_MID_CASE(12)
+      BDDA_MID_CASE(14) BDDA_MID_CASE(16)
+#undef BDDA_MID_CASE
+      default: break;
+    }
+  }
+}
+
+// Launch hook of a compile-time-specialised pencil kernel.
+typedef int (*FixedLaunchFn)(const PassArgs& a, int64_t P0, cudaStream_t st);
+struct FixedKernel {
+  int prec, kind, lt;
+  int r[4];            // radix sequence, padded with 1
+  FixedLaunchFn fn;
+};
+const FixedKernel* fixed_table_a(int* n);
+const FixedKernel* fixed_table_b(int* n);
+
+
+}  // namespace bdda

@@ -10,6 +10,8 @@
  *    as void*; NULL = legacy default stream).  Solver entry points read the
  *    residual back every iteration and therefore synchronise that stream.
  *  - Complex arrays are interleaved (re, im): c128 = 2 x double, c64 = 2 x float.
+ *  - The plan tables and Green's spectra must be 16-byte aligned (they are
+ *    staged into shared memory with 16-byte asynchronous copies).
  *  - Block vectors are row-major (3*N_occ, L): row 3m+c is component c of
  *    occupied dipole m, the L columns are orientations (reference layout,
  *    bl_krylov/bl_krylov.py:27-55).  Full-cuboid vectors are (3*Nc, L) with
@@ -77,6 +79,16 @@ int bdda_plan_radices(const bdda_plan* plan, int axis, int radices[12], int* nst
  * bdda_plan_table_bytes(); the plan uploads into it and keeps the pointer. */
 size_t bdda_plan_table_bytes(const bdda_plan* plan);
 int bdda_plan_attach_tables(bdda_plan* plan, void* dev_tables, void* stream);
+
+/* Launch shape of the pencil passes (no counterpart in the reference; used by
+ * the autotuner).  kind: 0 forward passes (Z, Y), 1 X pass (forward, Green
+ * multiply, inverse), 2 inverse passes (Y^-1, Z^-1).  smem_budget bounds the
+ * shared memory of one CTA and so selects the widest column tile that fits;
+ * threads per CTA is a multiple of 32 up to 512.  Process-wide settings. */
+int bdda_tune_set(int prec, int kind, size_t smem_budget, int threads);
+int bdda_tune_get(int prec, int kind, size_t* smem_budget, int* threads);
+/* on != 0 (default): radix sequences with a compile-time-specialised kernel use it */
+int bdda_tune_fixed(int on);
 
 /* ---- Green's tensor spectrum ----------------------------------------------
  * A'(r) (mvp_fft/mvp_fft.py:77-84) on the cyclic grid, 6 unique components

@@ -65,17 +65,28 @@ def smooth7(m):
     return m == 1
 
 
-@pytest.mark.parametrize("n", [(28, 28, 28), (17, 17, 17), (93, 112, 174), (5, 6, 7), (1, 1, 1), (11, 13, 37)])
+@pytest.mark.parametrize("n", [(28, 28, 28), (17, 17, 17), (93, 112, 174), (5, 6, 7), (1, 1, 1),
+                               (11, 13, 37), (3, 2, 4), (64, 100, 215)])
 def test_plan_grid_choice(n):
+    """Each axis gets an even 7-smooth length >= 2N factored into radices <= 10;
+    the x axis (fused Green multiply) ends with a radix <= 4; lengths stay
+    within 2N + 2N/4."""
     st, m, rad = _plan(n)
     assert st == _lib.OK
-    for N, M, r in zip(n, m, rad):
-        assert M >= 2 * N and M % 2 == 0 and smooth7(M)
-        if smooth7(2 * N):
-            assert M == 2 * N          # the reference's doubled grid
-        assert int(np.prod(r)) == M and set(r) <= {2, 3, 4, 5, 7, 8}
-        # nothing smaller qualifies
-        assert not any(smooth7(x) for x in range(2 * N, M, 2))
+    for a, (N, M, r) in enumerate(zip(n, m, rad)):
+        assert 2 * N <= M <= 2 * N + (2 * N) // 4 + 2 and M % 2 == 0 and smooth7(M)
+        assert int(np.prod(r)) == M and set(r) <= {2, 3, 4, 5, 6, 7, 8, 9, 10}
+        assert r == sorted(r, reverse=True)
+        if a == 0:
+            assert r[-1] <= 4
+
+
+def test_plan_factorization_minimises_stages():
+    st, m, rad = _plan((93, 112, 174), (192, 224, 350))
+    assert st == _lib.OK
+    assert [len(r) for r in rad] == [3, 3, 3]
+    st, m, rad = _plan((28, 28, 28), (56, 56, 56))
+    assert rad[1] == [8, 7] and rad[0][-1] <= 4
 
 
 def test_plan_accepts_explicit_grid_and_rejects_short_or_rough():
