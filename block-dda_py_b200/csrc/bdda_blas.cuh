@@ -73,6 +73,7 @@ struct DotArgs {
 };
 
 // Host-side launchers (bdda_blas.cu)
+void set_fixed_blas(int on);
 template <typename T> int gram(const GramArgs& g, bool conj, double2* out, cudaStream_t st);
 template <typename T> int update(const UpdateArgs& u, cudaStream_t st);
 template <typename T> int dots(const DotArgs& d, cudaStream_t st);

@@ -19,6 +19,7 @@
 
 #include "bdda_internal.h"
 
+#include "bdda_blas.cuh"
 #include "bdda_pencil.cuh"
 
 namespace bdda {
@@ -425,6 +426,7 @@ int bdda_tune_set(int prec, int kind, size_t smem_budget, int threads) {
 
 int bdda_tune_fixed(int on) {
   g_use_fixed = on ? 1 : 0;
+  set_fixed_blas(on);
   return BDDA_OK;
 }
 

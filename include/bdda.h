@@ -87,7 +87,8 @@ int bdda_plan_attach_tables(bdda_plan* plan, void* dev_tables, void* stream);
  * threads per CTA is a multiple of 32 up to 512.  Process-wide settings. */
 int bdda_tune_set(int prec, int kind, size_t smem_budget, int threads);
 int bdda_tune_get(int prec, int kind, size_t* smem_budget, int* threads);
-/* on != 0 (default): radix sequences with a compile-time-specialised kernel use it */
+/* on != 0 (default): radix sequences and block widths L with a compile-time-
+ * specialised kernel use it (FFT passes, Gram products, block updates) */
 int bdda_tune_fixed(int on);
 
 /* ---- Green's tensor spectrum ----------------------------------------------

@@ -157,3 +157,25 @@ def test_duplicate_columns_raise_linalgerror(mods):
     with pytest.raises(np.linalg.LinAlgError):
         O.bicgstab(g["n"], 3, g["address"], O.fft_init(g["n"], 3, float(g["lf"]), float(g["k"])),
                    g["diag_A"], B, 1e-5, 50)
+
+
+@pytest.mark.parametrize("L", [16, 32, 64])
+@pytest.mark.parametrize("solver", ["bicgstab", "cocg"])
+def test_specialised_block_kernels_match_generic(mods, L, solver):
+    """The L-specialised Gram / update kernels and the generic ones give the same solve."""
+    from bdda_b200 import _lib
+    mf, bk = mods
+    rec = load_geometry(os.path.join(GOLDEN, "kat_test_dda.npz"))
+    n, lf, address, pos, geom, eper_r, diag, B = _case(rec)
+    rng = np.random.default_rng(L)
+    Bl = rng.standard_normal((B.shape[0], L)) + 1j * rng.standard_normal((B.shape[0], L))
+    til = mf.fft_init(n, 3, lf, geom["k"])
+    fn = solver_fn(bk, solver)
+    X1, it1, err1 = fn(n, 3, address, til, diag, Bl, 1e-6, 60)
+    _lib.load().bdda_tune_fixed(0)
+    try:
+        X2, it2, err2 = fn(n, 3, address, til, diag, Bl, 1e-6, 60)
+    finally:
+        _lib.load().bdda_tune_fixed(1)
+    assert err1 < 1e-6 and err2 < 1e-6 and abs(it1 - it2) <= 1
+    assert rel(X1, X2) < 1e-5
