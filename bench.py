@@ -10,7 +10,12 @@ model and shipped in tests/golden/geometry_cfg2.npz), birefringent m_p =
 (seed 2).  One step = polarizability + right-hand side + block solve to
 ||R||/||M^-1 B|| < 1e-5 + observables, for all 64 orientations.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl bdda|reference] [--form fp64]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl bdda|reference] [--form mixed|fp64]
+
+The headline (default) form runs the block solves in complex64 inside an
+FP64 iterative refinement to the true residual 1e-5; the plain complex128
+path is timed beside it ("plain_fp64"), with the error of every observable
+against it.
 
 Prints one JSON line on rank 0.  Multi-GPU runs are replicas (each rank
 solves its own copy; there is no data exchange on this path).
@@ -140,12 +145,13 @@ def run_bdda(args, rank, world, local_rank):
     lib = _lib.load()
     L = args.L
     geo, euler = load_workload(L)
+    mixed = args.form == "mixed"
 
-    def make_dd():
+    def make_dd(precision):
         t = sc.Target("gre", geo["lattice_n"], geo["lattice_lf"], geo["grid"], geo["is_in"], geo["m_p_xyz"])
         dd = sc.DiscreteDipoles(t, sc.IncidentField(float(geo["wl_0"]), float(geo["m_m"]), euler))
         dd.tol, dd.itermax = TOL, ITERMAX
-        dd.precision = None if args.form == "fp64" else args.form
+        dd.precision = precision
         return dd
 
     def barrier():
@@ -161,43 +167,75 @@ def run_bdda(args, rank, world, local_rank):
         return float(t.item())
 
     # ---- set-up (untimed): resident geometry and Green's spectrum ----
-    dd = make_dd()
+    dd = make_dd("mixed" if mixed else None)
     t0 = time.perf_counter()
     dd.set_interaction_matrix()
     torch.cuda.synchronize()
     green_s = time.perf_counter() - t0
     green = dd.Au_til
 
-    def device_step():
-        dd.set_interaction_matrix(green=green)
-        dd.solve_matrix_equation()
-        return dd.observables()
+    def device_step(d):
+        d.set_interaction_matrix(green=green)
+        d.solve_matrix_equation()
+        return d.observables()
 
-    for _ in range(args.warmup):
-        device_step()
-    iters = dd.iter_fin + 1
-    converged = dd.converge
-    n0 = lib.bdda_launch_count()
-    lib.bdda_profile_enable(1)
-    barrier()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local_rank) as clk:
+    def timed(d, steps, sampler=None):
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        for _ in range(args.steps):
-            device_step()
+        for _ in range(steps):
+            out = device_step(d)
         e1.record()
         barrier()
-    ms = max_over_ranks(e0.elapsed_time(e1) / args.steps)
+        return max_over_ranks(e0.elapsed_time(e1) / steps), out
+
+    for _ in range(args.warmup):
+        device_step(dd)
+    n0 = lib.bdda_launch_count()
+    lib.bdda_profile_enable(1)
+    with ClockSampler(local_rank) as clk:
+        ms, obs = timed(dd, args.steps)
     launches = (lib.bdda_launch_count() - n0) / args.steps
-    pass_ms = (_lib.C.c_double * 5)()
-    nmvp = _lib.C.c_longlong(0)
-    lib.bdda_profile_read(pass_ms, _lib.C.byref(nmvp))
+    prof = {}
+    for prec in (_lib.C128, _lib.C64):
+        pm = (_lib.C.c_double * 5)()
+        nm = _lib.C.c_longlong(0)
+        lib.bdda_profile_read(prec, pm, _lib.C.byref(nm))
+        if nm.value:
+            prof[prec] = ([pm[i] / nm.value for i in range(5)], nm.value)
     lib.bdda_profile_enable(0)
     clocks = clk.summary()
+    iters = dd.iter_fin + 1
+
+    # ---- the plain FP64 path beside it (the metric's comparison) ----
+    plain = None
+    if mixed and not args.no_fp64:
+        d64 = make_dd(None)
+        device_step(d64)
+        ms64, obs64 = timed(d64, args.steps)
+        # converged FP64 solution (tol 1e-10), untimed: the accuracy reference
+        dref = make_dd(None)
+        dref.tol, dref.itermax = 1e-10, 400
+        obsref = device_step(dref)
+
+        def rel_errs(o, r):
+            out = {}
+            for name, cols in (("C_ext", (1,)), ("S_fw_theta", (2, 3)), ("S_fw_phi", (4, 5)),
+                               ("S_bk", (10, 11))):
+                a = o[:, cols[0]] + (1j * o[:, cols[1]] if len(cols) > 1 else 0)
+                b = r[:, cols[0]] + (1j * r[:, cols[1]] if len(cols) > 1 else 0)
+                out[name] = float("%.3g" % (np.max(np.abs(a - b)) / np.max(np.abs(b))))
+            return out
+        plain = {"value": round(world * L / (ms64 * 1e-3), 3), "unit": "orientations/s",
+                 "ms_per_step": round(ms64, 3), "iterations": d64.iter_fin + 1,
+                 "speedup_of_mixed": round(ms64 / ms, 3),
+                 "max_rel_err_mixed_vs_fp64": rel_errs(obs, obs64),
+                 "max_rel_err_vs_converged_fp64": {"mixed": rel_errs(obs, obsref),
+                                                   "fp64_tol1e-5": rel_errs(obs64, obsref)}}
 
     # ---- end to end through the public API, host numpy in and out ----
     def e2e_step():
-        d = make_dd()
+        d = make_dd("mixed" if mixed else None)
         d.set_interaction_matrix()
         d.solve_matrix_equation()
         res = (d.compute_C_abs(), d.compute_C_ext(), d.compute_PCAS_observable_S_fw(),
@@ -215,10 +253,8 @@ def run_bdda(args, rank, world, local_rank):
     h2d += d_e2e._dev["occ"].address_dev.numel() * 8
     d2h = L * 12 * 8
 
-    # ---- roofline of the product (measured above over the timed region) ----
+    # ---- roofline of the dominant kernel chain (measured over the timed region) ----
     plan = green.plan
-    s = 16 if args.form == "fp64" else 8
-    pb = mvp_pass_bytes(plan.n, plan.m, dd.num_element_occupy, L, s)
     peaks = {}
     try:
         with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
@@ -227,13 +263,25 @@ def run_bdda(args, rank, world, local_rank):
         pass
     peak = float(peaks.get("hbm_gbs", 6650.0))
     peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
-    n_mvp = max(1, nmvp.value)
-    per_pass_ms = [pass_ms[i] / n_mvp for i in range(5)]
-    mvp_ms = sum(per_pass_ms)
-    achieved = sum(pb) / (mvp_ms * 1e-3) / 1e9
-    passes = [{"pass": nm, "ms": round(t, 3), "GB/s": round(b / (t * 1e-3) / 1e9, 1),
-               "frac": round(b / (t * 1e-3) / 1e9 / peak, 3)}
-              for nm, t, b in zip(["Z", "Y", "X", "Y^-1", "Z^-1"], per_pass_ms, pb)]
+    lines = {}
+    for prec, (per, cnt) in prof.items():
+        s = 16 if prec == _lib.C128 else 8
+        pb = mvp_pass_bytes(plan.n, plan.m, dd.num_element_occupy, L, s)
+        mvp_ms = sum(per)
+        lines[prec] = {"alg_bytes_per_mvp": int(sum(pb)), "mvp_ms": round(mvp_ms, 3), "mvps_timed": cnt,
+                       "achieved": round(sum(pb) / (mvp_ms * 1e-3) / 1e9, 1),
+                       "passes": [{"pass": nm, "ms": round(tm, 3), "GB/s": round(b / (tm * 1e-3) / 1e9, 1),
+                                   "frac": round(b / (tm * 1e-3) / 1e9 / peak, 3)}
+                                  for nm, tm, b in zip(["Z", "Y", "X", "Y^-1", "Z^-1"], per, pb)]}
+    main = _lib.C64 if (mixed and _lib.C64 in lines) else _lib.C128
+    rl = lines[main]
+    roofline = {"kernel": "block MVP, %s (5 pencil passes)" % ("complex64" if main == _lib.C64 else "complex128"),
+                "bound": "hbm", "achieved": rl["achieved"], "peak": peak, "unit": "GB/s",
+                "frac": round(rl["achieved"] / peak, 3), "traffic": None, "peak_source": peak_src,
+                "alg_bytes_per_mvp": rl["alg_bytes_per_mvp"], "mvp_ms": rl["mvp_ms"],
+                "mvps_timed": rl["mvps_timed"], "passes": rl["passes"]}
+    if mixed and _lib.C128 in lines:
+        roofline["complex128_mvp"] = {k: lines[_lib.C128][k] for k in ("achieved", "mvp_ms", "mvps_timed")}
 
     result = {
         "metric": METRIC,
@@ -242,22 +290,20 @@ def run_bdda(args, rank, world, local_rank):
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(ms, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "complex128" if args.form == "fp64" else "complex64+complex128",
+        "dtype": "complex64 Krylov + complex128 refinement" if mixed else "complex128",
         "form": args.form,
         "data": "synthetic: reference GRE geometry (seed 1) and SO(3) orientations (seed 2)",
         "config": dict(workload_config(L), parallelism="replicas x%d" % world,
-                       green_build_s=round(green_s, 4), iterations=iters, converged=converged),
+                       green_build_s=round(green_s, 4), iterations=iters, converged=dd.converge,
+                       true_residual=dd.err_fin if mixed else None),
+        "plain_fp64": plain,
         "e2e": {"value": round(world * L / e2e_s, 3), "unit": "orientations/s",
                 "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                 "includes": "Target/IncidentField/DiscreteDipoles from host arrays, Green build, solve, "
                             "observables to host"},
         "gpu_launches": int(round(launches)),
         "clocks": clocks,
-        "roofline": {"kernel": "block MVP (5 pencil passes)", "bound": "hbm",
-                     "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                     "frac": round(achieved / peak, 3), "traffic": None, "peak_source": peak_src,
-                     "alg_bytes_per_mvp": int(sum(pb)), "mvp_ms": round(mvp_ms, 3), "mvps_timed": n_mvp,
-                     "passes": passes},
+        "roofline": roofline,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         result["cpu_baseline"] = cpu_reference(geo, L, sample_iters=1)
@@ -355,7 +401,7 @@ def run_mvp_only(args):
     torch.cuda.synchronize()
     pass_ms = (_lib.C.c_double * 5)()
     nm = _lib.C.c_longlong(0)
-    lib.bdda_profile_read(pass_ms, _lib.C.byref(nm))
+    lib.bdda_profile_read(-1, pass_ms, _lib.C.byref(nm))
     lib.bdda_profile_enable(0)
     s = 16 if prec == _lib.C128 else 8
     pb = mvp_pass_bytes(plan.n, plan.m, occ.n_occ, args.L, s)
@@ -373,7 +419,9 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="bdda", choices=["bdda", "reference"])
-    ap.add_argument("--form", default="fp64", choices=["fp64", "fp32"])
+    ap.add_argument("--form", default="mixed", choices=["mixed", "fp64", "fp32"],
+                    help="mixed: FP32 block solves inside FP64 refinement (headline); fp64: plain complex128")
+    ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 comparison run")
     ap.add_argument("--L", type=int, default=64)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--mvp-only", action="store_true", help="time block MVPs of the workload only")

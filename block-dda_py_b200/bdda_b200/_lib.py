@@ -53,12 +53,15 @@ PROTOTYPES = {
     "bdda_fft_mvp": (_i, [_vp, _i, _i, _vp, _vp, _vp, _vp, _vp]),
     "bdda_block_mvp": (_i, [_vp, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "bdda_solver_workspace_bytes": (_sz, [_vp, _i, _i, _i, _i]),
+    "bdda_refine_workspace_bytes": (_sz, [_vp, _i, _i]),
+    "bdda_refine_solve": (_i, [_vp, _i, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _d, _i, _d, _i, _vp, _pi,
+                               C.POINTER(_d), C.POINTER(_d), _vp, _sz, _vp]),
     "bdda_polarizability": (_i, [_i, C.POINTER(_d), _d, _d, _d, _vp, _vp, _vp]),
     "bdda_incident_rhs": (_i, [_i, _i, _d, _vp, _vp, _vp, _vp, _vp]),
     "bdda_observables_workspace_bytes": (_sz, [_i]),
     "bdda_launch_count": (C.c_ulonglong, []),
     "bdda_profile_enable": (_i, [_i]),
-    "bdda_profile_read": (_i, [C.POINTER(_d), C.POINTER(C.c_longlong)]),
+    "bdda_profile_read": (_i, [_i, C.POINTER(_d), C.POINTER(C.c_longlong)]),
     "bdda_observables": (_i, [_i, _i, _d, _d, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "bdda_solve": (_i, [_vp, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _vp, _d, _i, _vp, _pi,
                         C.POINTER(_d), C.POINTER(_d), _vp, _sz, _vp]),

@@ -58,14 +58,19 @@ def _block_mvp(n, f, Au_til, full_idx, DIAG_A, S, jpre, precision=None):
     return out.cpu().numpy() if to_numpy else out
 
 
+MIXED = ("mixed", "c64-refine", "fp32-refine", "mixed-reliable")
+
+
 def _solve(kind, n, f, address, Au_til, DIAG_A, B, tol, itermax, X0=None, precision=None,
-           history=None, verbose=False):
-    """Shared body of the two block solvers (C entry point ``bdda_solve``)."""
+           history=None, verbose=False, inner_tol=1e-4, max_outer=20):
+    """Shared body of the block solvers (C entry points ``bdda_solve`` / ``bdda_refine_solve``)."""
     if f != 3:
         raise ValueError("only f=3 (electric dipoles) is supported.")
     g = as_green(n, Au_til)
     plan = g.plan
-    prec = precision_code(precision)
+    mixed = isinstance(precision, str) and precision.lower() in MIXED
+    reliable = mixed and precision.lower() == "mixed-reliable" and kind == _lib.BICGSTAB
+    prec = _lib.C128 if mixed else precision_code(precision)
     occ = address if isinstance(address, Occupancy) else Occupancy(plan, address)
     to_numpy = not isinstance(B, torch.Tensor)
     Bd = to_device(B, torch.complex128, plan.device)
@@ -80,16 +85,28 @@ def _solve(kind, n, f, address, Au_til, DIAG_A, B, tol, itermax, X0=None, precis
     X0d = None if X0 is None else to_device(X0, torch.complex128, plan.device).reshape(Bd.shape).contiguous()
     lib = _lib.load()
     X = torch.empty_like(Bd)
-    nbytes = int(lib.bdda_solver_workspace_bytes(plan.handle, kind, prec, L, occ.n_occ))
-    work = torch.empty(max(nbytes, 16), dtype=torch.uint8, device=plan.device)
     itermax = int(itermax)
     hist = (C.c_double * max(itermax, 1))()
     it = C.c_int(0)
     err = C.c_double(float("inf"))
-    status = lib.bdda_solve(plan.handle, kind, prec, L, occ.n_occ, ptr(g.ghat(prec)), ptr(occ.cell_map),
-                            ptr(diag), ptr(Bd), ptr(X0d), float(tol), itermax, ptr(X), C.byref(it),
-                            C.byref(err), hist, ptr(work), nbytes, stream_ptr(plan.device))
-    _lib.check(status, "bdda_solve")
+    if mixed:
+        nbytes = int(lib.bdda_refine_workspace_bytes(plan.handle, L, occ.n_occ))
+        work = torch.empty(max(nbytes, 16), dtype=torch.uint8, device=plan.device)
+        status = lib.bdda_refine_solve(plan.handle, kind, L, occ.n_occ, ptr(g.ghat(_lib.C128)),
+                                       ptr(g.ghat(_lib.C64)), ptr(occ.cell_map), ptr(diag), ptr(Bd), ptr(X0d),
+                                       float(tol), itermax,
+                                       float(1e-2 if reliable else inner_tol),
+                                       -abs(int(max_outer)) if reliable else abs(int(max_outer)), ptr(X),
+                                       C.byref(it), C.byref(err), hist, ptr(work), nbytes,
+                                       stream_ptr(plan.device))
+        _lib.check(status, "bdda_refine_solve")
+    else:
+        nbytes = int(lib.bdda_solver_workspace_bytes(plan.handle, kind, prec, L, occ.n_occ))
+        work = torch.empty(max(nbytes, 16), dtype=torch.uint8, device=plan.device)
+        status = lib.bdda_solve(plan.handle, kind, prec, L, occ.n_occ, ptr(g.ghat(prec)), ptr(occ.cell_map),
+                                ptr(diag), ptr(Bd), ptr(X0d), float(tol), itermax, ptr(X), C.byref(it),
+                                C.byref(err), hist, ptr(work), nbytes, stream_ptr(plan.device))
+        _lib.check(status, "bdda_solve")
     ran = 0 if itermax == 0 else it.value + 1
     if history is not None:
         history.extend(hist[i] for i in range(ran))
@@ -101,25 +118,30 @@ def _solve(kind, n, f, address, Au_til, DIAG_A, B, tol, itermax, X0=None, precis
 
 
 def bl_cocg_rq_jacobi_mvp_fft(n, f, address, Au_til, DIAG_A, B, tol, itermax, X0=None,
-                              precision=None, history=None, verbose=False):
+                              precision=None, history=None, verbose=False, inner_tol=1e-4, max_outer=20):
     """Block-COCG-rq with Jacobi preconditioning (bl_krylov.py:58-118).
 
     Returns ``(X, iter_fin, err_fin)`` with the reference's meaning: X the
     (f*N_occ, L) solution, iter_fin the 0-based index of the last iteration,
     err_fin = ||xi||_F / ||M^-1 B||_F at that iteration.  Not converging is
     not an error.  Extra keywords (all optional): ``X0`` initial guess,
-    ``precision`` "c128" (default) or "c64", ``history`` list receiving the
-    per-iteration residuals, ``verbose`` prints them like the reference.
+    ``precision`` "c128" (default), "c64" (FP32 throughout), "mixed" (FP32
+    block solves restarted inside an FP64 iterative refinement; err_fin is
+    then the true residual ||M^-1 (B - A X)|| / ||M^-1 B||; ``inner_tol``
+    and ``max_outer`` tune it) or, for BiCGSTAB, "mixed-reliable" (one FP32
+    recursion with FP64 residual replacement, for small L), ``history``
+    list receiving the per-iteration residuals, ``verbose`` prints them like
+    the reference.
     The QR factorisations are CholeskyQR (R with real positive diagonal
     instead of LAPACK's Householder signs); X and err are independent of
     that choice.
     """
     return _solve(_lib.COCG_RQ, n, f, address, Au_til, DIAG_A, B, tol, itermax, X0, precision,
-                  history, verbose)
+                  history, verbose, inner_tol, max_outer)
 
 
 def bl_bicgstab_jacobi_mvp_fft(n, f, address, Au_til, DIAG_A, B, tol, itermax, X0=None,
-                               precision=None, history=None, verbose=False):
+                               precision=None, history=None, verbose=False, inner_tol=1e-4, max_outer=20):
     """Block-BiCGSTAB with Jacobi preconditioning (bl_krylov.py:121-187).
 
     Returns ``(X, iter_fin, err_fin)`` as the reference; err_fin is the
@@ -128,4 +150,4 @@ def bl_bicgstab_jacobi_mvp_fft(n, f, address, Au_til, DIAG_A, B, tol, itermax, X
     :func:`bl_cocg_rq_jacobi_mvp_fft`.
     """
     return _solve(_lib.BICGSTAB, n, f, address, Au_til, DIAG_A, B, tol, itermax, X0, precision,
-                  history, verbose)
+                  history, verbose, inner_tol, max_outer)

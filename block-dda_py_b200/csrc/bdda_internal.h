@@ -26,7 +26,8 @@ namespace bdda {
 void count_launch(int n = 1);
 // Optional per-pass timing of every block MVP (events on the launching stream).
 bool profiling();
-void profile_mark(int pass, cudaStream_t st);   // pass 0..5: before Z, after Z, Y, X, Y^-1, Z^-1
+// pass 0..5: before Z, after Z, Y, X, Y^-1, Z^-1; prec tags the product (0 c128, 1 c64)
+void profile_mark(int pass, cudaStream_t st, int prec = 0);
 
 #define BDDA_CUDA_TRY(expr)                      \
   do {                                           \

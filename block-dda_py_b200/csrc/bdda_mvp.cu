@@ -187,7 +187,7 @@ static int run_mvp(const bdda_plan* plan, int L, const T* ghat, const int32_t* c
   b.C = C;
   b.scale = 1.0;
   const bool prof = profiling();
-  if (prof) profile_mark(0, st);
+  if (prof) profile_mark(0, st, prec_of<T>());
 
   {  // Z: gather + forward z
     PassArgs a = b;

@@ -17,12 +17,14 @@ static std::atomic<bool> g_profiling{false};
 static std::mutex g_mu;
 static std::vector<cudaEvent_t> g_free;
 static std::vector<cudaEvent_t> g_marks[6];
+static std::vector<int> g_prec;   // precision of each recorded product
 
 void count_launch(int n) { g_launches.fetch_add((unsigned long long)n, std::memory_order_relaxed); }
 bool profiling() { return g_profiling.load(std::memory_order_relaxed); }
 
-void profile_mark(int pass, cudaStream_t st) {
+void profile_mark(int pass, cudaStream_t st, int prec) {
   std::lock_guard<std::mutex> lk(g_mu);
+  if (pass == 0) g_prec.push_back(prec);
   cudaEvent_t e;
   if (!g_free.empty()) {
     e = g_free.back();
@@ -48,18 +50,23 @@ int bdda_profile_enable(int on) {
     for (cudaEvent_t e : g_marks[p]) g_free.push_back(e);
     g_marks[p].clear();
   }
+  g_prec.clear();
   g_profiling.store(on != 0);
   return BDDA_OK;
 }
 
-int bdda_profile_read(double pass_ms[5], long long* n_mvp) {
+int bdda_profile_read(int prec, double pass_ms[5], long long* n_mvp) {
   if (!pass_ms || !n_mvp) return BDDA_BAD_ARG;
   std::lock_guard<std::mutex> lk(g_mu);
   const size_t n = g_marks[0].size();
   for (int p = 1; p < 6; ++p)
     if (g_marks[p].size() != n) return BDDA_BAD_ARG;
+  if (g_prec.size() != n) return BDDA_BAD_ARG;
   for (int p = 0; p < 5; ++p) pass_ms[p] = 0.0;
+  long long counted = 0;
   for (size_t i = 0; i < n; ++i) {
+    if (prec >= 0 && g_prec[i] != prec) continue;
+    ++counted;
     BDDA_CUDA_TRY(cudaEventSynchronize(g_marks[5][i]));
     for (int p = 0; p < 5; ++p) {
       float ms = 0.f;
@@ -67,7 +74,7 @@ int bdda_profile_read(double pass_ms[5], long long* n_mvp) {
       pass_ms[p] += ms;
     }
   }
-  *n_mvp = (long long)n;
+  *n_mvp = counted;
   return BDDA_OK;
 }
 

@@ -562,6 +562,283 @@ static int run_solver(int solver, const bdda_plan* p, int L, int n_occ, const vo
   return status;
 }
 
+// ---- FP32 Krylov with FP64 iterative refinement -----------------------------------
+// Outer loop in complex128: r = M^-1 (B - A X) with the FP64 product; inner
+// block solve of M^-1 A D = r in complex64 (FP32 product and vectors, FP64
+// Gram / small solves); X += D in FP64.  Stops when the true relative
+// residual ||r|| / ||M^-1 B|| < tol.
+struct RLayout {
+  size_t field, v64[4], diag64, jpre64, v32[kVecs], diag32, jpre32, partial, small, st64, st32, total;
+};
+
+static RLayout rlayout(const bdda_plan* p, int L, int n_occ) {
+  RLayout o;
+  const size_t v64 = (size_t)3 * n_occ * L * 16, v32 = (size_t)3 * n_occ * L * 8;
+  size_t off = 0;
+  o.field = off; off = al(off + bdda_mvp_workspace_bytes(p, BDDA_C128, L));   // shared by both precisions
+  for (int v = 0; v < 4; ++v) { o.v64[v] = off; off = al(off + v64); }
+  o.diag64 = off; off = al(off + (size_t)3 * n_occ * 16);
+  o.jpre64 = off; off = al(off + (size_t)3 * n_occ * 16);
+  for (int v = 0; v < kVecs; ++v) { o.v32[v] = off; off = al(off + v32); }
+  o.diag32 = off; off = al(off + (size_t)3 * n_occ * 8);
+  o.jpre32 = off; off = al(off + (size_t)3 * n_occ * 8);
+  o.partial = off; off = al(off + (size_t)kRedBlocks * 2 * kMaxL * kMaxL * sizeof(double2));
+  o.small = off; off = al(off + (size_t)kSmallMats * kMaxL * kMaxL * sizeof(double2) + 64 * sizeof(int));
+  o.st64 = off; off = al(off + sizeof(SolverState));
+  o.st32 = off; off = al(off + sizeof(SolverState));
+  o.total = off;
+  return o;
+}
+
+__global__ void accumulate_kernel(double2* X, const float2* D, int64_t n) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const float2 d = D[i];
+    X[i] = make_double2(X[i].x + (double)d.x, X[i].y + (double)d.y);
+  }
+}
+
+__global__ void negate_accumulate_kernel(double2* X, const float2* D, int64_t n) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const float2 d = D[i];
+    X[i] = make_double2(X[i].x - (double)d.x, X[i].y - (double)d.y);
+  }
+}
+
+template <typename T>
+static void fill_ctx(Ctx<T>& c, const bdda_plan* p, int L, int n_occ, const void* ghat, const int32_t* cell_map,
+                     unsigned char* w, size_t field, size_t diag, size_t jpre, const size_t* vecs, int nvec,
+                     size_t partial, size_t small, size_t state, cudaStream_t st) {
+  c.plan = p;
+  c.L = L;
+  c.n = 3 * (int64_t)n_occ;
+  c.ghat = static_cast<const T*>(ghat);
+  c.cell_map = cell_map;
+  c.field = reinterpret_cast<T*>(w + field);
+  for (int v = 0; v < kVecs; ++v) c.vec[v] = v < nvec ? reinterpret_cast<T*>(w + vecs[v]) : nullptr;
+  c.diag = reinterpret_cast<T*>(w + diag);
+  c.jpre = reinterpret_cast<T*>(w + jpre);
+  c.partial = reinterpret_cast<double2*>(w + partial);
+  c.sp = small_ptrs(w + small);
+  c.st = reinterpret_cast<SolverState*>(w + state);
+  c.stream = st;
+  c.sm2 = (size_t)2 * L * L * sizeof(double2);
+  c.sm3 = (size_t)3 * L * L * sizeof(double2);
+}
+
+// Block-BiCGSTAB in complex64 with FP64 reliable updates (residual
+// replacement, van der Vorst & Ye): the Krylov vectors and products are FP32,
+// the solution X is accumulated in FP64 (X += P alpha + zeta T, the increment
+// formed in FP32), and whenever the recursive residual has dropped by the
+// factor kReplace since the last replacement -- and before declaring convergence --
+// R is replaced by the true residual M^-1 (B - A X) from the FP64 product.
+// The Krylov space is kept, so nothing is lost to restarts; convergence is
+// judged on the true residual.
+static int bicgstab_reliable(Ctx<double2>& c64, Ctx<float2>& c32, bool has_x0, double tol, int itermax,
+                             double kReplace, int* iter_fin, double* err_fin, double* hist) {
+  double2 *Bj = c64.vec[0], *X = c64.vec[1], *R64 = c64.vec[2], *Tm = c64.vec[3];
+  float2 *U = c32.vec[0], *R = c32.vec[1], *P = c32.vec[2], *R0 = c32.vec[3], *V = c32.vec[4],
+         *Tt = c32.vec[5], *Z = c32.vec[6];
+  const int L = c32.L;
+  const int64_t ne = c64.n * L;
+  const cudaStream_t st = c64.stream;
+  double* dot_partial = reinterpret_cast<double*>(c32.partial) + 2 * (size_t)kMaxL * kMaxL * kRedBlocks;
+  // true residual into R64 / R (and its norm into c64.st)
+  auto replace = [&](double* err) -> int {
+    TRY(mvp<double2>(c64, X, Tm));
+    TRY(upd<double2>(c64, R64, Bj, nullptr, Tm, c64.sp.r, nullptr, nullptr, nullptr, nullptr, true));
+    norm_kernel<<<1, 256, 0, st>>>(reinterpret_cast<double*>(c64.partial), kRedBlocks, c64.st, 0);
+    convert_in_kernel<float2><<<kRedBlocks, 256, 0, st>>>(R64, R, ne);
+    count_launch(2);
+    int bad = 0;
+    TRY(read_state(c64, err, &bad));
+    return bad == 2 ? BDDA_NOT_CONVERGED : BDDA_OK;
+  };
+  TRY(upd<double2>(c64, Tm, Bj, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, true));
+  norm_kernel<<<1, 256, 0, st>>>(reinterpret_cast<double*>(c64.partial), kRedBlocks, c64.st, 1);
+  count_launch();
+  double err = INFINITY;
+  if (has_x0) {
+    if (replace(&err) != BDDA_OK) return BDDA_NOT_CONVERGED;
+  } else {
+    BDDA_CUDA_TRY(cudaMemsetAsync(X, 0, (size_t)ne * sizeof(double2), st));
+    convert_in_kernel<float2><<<kRedBlocks, 256, 0, st>>>(Bj, R, ne);
+    count_launch();
+    err = 1.0;
+  }
+  // the FP32 recursion runs on the residual scaled to the state's norm
+  TRY(upd<float2>(c32, P, R, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, true));
+  norm_kernel<<<1, 256, 0, st>>>(reinterpret_cast<double*>(c32.partial), kRedBlocks, c32.st, 1);
+  count_launch();
+  TRY(upd<float2>(c32, R0, R, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, false));
+  double last = err;           // true residual at the last replacement (relative to ||M^-1 B||)
+  const double base = err;     // ||R|| at the start of the FP32 recursion, relative to ||M^-1 B||
+  *iter_fin = 0;
+  *err_fin = err;
+  if (err < tol) return BDDA_OK;
+  double scale = base;         // recursion residual (relative to its start) -> relative to ||M^-1 B||
+  for (int k = 0; k < itermax; ++k) {
+    TRY(mvp<float2>(c32, P, V));
+    TRY(gram2<float2>(c32, true, R0, V, R, c32.sp.g2));
+    bicg_alpha_kernel<<<1, 256, c32.sm2, st>>>(c32.sp, L, c32.st);
+    count_launch();
+    TRY(upd<float2>(c32, Tt, R, nullptr, nullptr, nullptr, V, nullptr, nullptr, c32.sp.negalpha, false));
+    TRY(mvp<float2>(c32, Tt, Z));
+    TRY(gram2<float2>(c32, true, R0, Z, nullptr, c32.sp.g2));
+    DotArgs d;
+    d.n = c32.n * L; d.A = Z; d.B = Tt; d.partial = dot_partial;
+    TRY(dots<float2>(d, st));
+    bicg_zeta_beta_kernel<<<1, 256, c32.sm2, st>>>(c32.sp, L, dot_partial, kRedBlocks, c32.st);
+    count_launch();
+    // X += P alpha + zeta T: increment in FP32, accumulation in FP64
+    TRY(upd<float2>(c32, U, nullptr, nullptr, Tt, &c32.st->zeta, P, nullptr, nullptr, c32.sp.alpha, false));
+    accumulate_kernel<<<kRedBlocks, 256, 0, st>>>(X, U, ne);
+    count_launch();
+    TRY(upd<float2>(c32, R, Tt, nullptr, Z, &c32.st->negzeta, nullptr, nullptr, nullptr, nullptr, true));
+    norm_kernel<<<1, 256, 0, st>>>(reinterpret_cast<double*>(c32.partial), kRedBlocks, c32.st, 0);
+    count_launch();
+    double rr = INFINITY;
+    int bad = 0;
+    TRY(read_state(c32, &rr, &bad));
+    if (bad == 1) return BDDA_BREAKDOWN;
+    err = rr * scale;
+    *iter_fin = k;
+    if (hist) hist[k] = err;
+    if (bad == 2) { *err_fin = err; return BDDA_NOT_CONVERGED; }
+    if (err < tol || err < kReplace * last) {
+      double tr = INFINITY;
+      if (replace(&tr) != BDDA_OK) { *err_fin = tr; return BDDA_NOT_CONVERGED; }
+      last = tr;
+      err = tr;
+      if (hist) hist[k] = err;
+      // the recursion continues from the true residual: rescale its norm bookkeeping
+      TRY(upd<float2>(c32, Tt, R, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, true));
+      norm_kernel<<<1, 256, 0, st>>>(reinterpret_cast<double*>(c32.partial), kRedBlocks, c32.st, 1);
+      count_launch();
+      scale = tr;
+      if (tr < tol) { *err_fin = tr; return BDDA_OK; }
+    }
+    *err_fin = err;
+    TRY(upd<float2>(c32, P, R, nullptr, nullptr, nullptr, P, V, &c32.st->negzeta, c32.sp.beta, false));
+  }
+  // report the true residual of the returned X
+  double tr = INFINITY;
+  if (replace(&tr) == BDDA_OK) *err_fin = tr;
+  return *err_fin < tol ? BDDA_OK : BDDA_NOT_CONVERGED;
+}
+
+static int run_refine(int solver, bool restart, const bdda_plan* p, int L, int n_occ, const void* ghat64,
+                      const void* ghat32, const int32_t* cell_map, const double2* diag, const double2* B,
+                      const double2* X0, double tol, int itermax, double inner_tol, int max_outer, double2* Xout,
+                      int* iter_fin, double* err_fin, double* hist, void* work, size_t work_bytes,
+                      cudaStream_t st) {
+  const RLayout o = rlayout(p, L, n_occ);
+  if (work_bytes < o.total) return BDDA_NO_WORKSPACE;
+  unsigned char* w = static_cast<unsigned char*>(work);
+  Ctx<double2> c64;
+  Ctx<float2> c32;
+  fill_ctx(c64, p, L, n_occ, ghat64, cell_map, w, o.field, o.diag64, o.jpre64, o.v64, 4, o.partial, o.small,
+           o.st64, st);
+  fill_ctx(c32, p, L, n_occ, ghat32, cell_map, w, o.field, o.diag32, o.jpre32, o.v32, kVecs, o.partial,
+           o.small, o.st32, st);
+  TRY(allow_smem(bicg_alpha_kernel, c32.sm2));
+  TRY(allow_smem(bicg_zeta_beta_kernel, c32.sm2));
+  TRY(allow_smem(cholqr_step_kernel, c32.sm2));
+  TRY(allow_smem(cocg_alpha_kernel, c32.sm3));
+  TRY(allow_smem(cocg_xi_kernel, c32.sm3));
+  TRY(allow_smem(cocg_beta_kernel, c32.sm3));
+  double2 *Bj = c64.vec[0], *X = c64.vec[1], *R = c64.vec[2], *Tm = c64.vec[3];
+  const int64_t ne = c64.n * L;
+  BDDA_CUDA_TRY(cudaMemsetAsync(c64.st, 0, sizeof(SolverState), st));
+  BDDA_CUDA_TRY(cudaMemsetAsync(c32.st, 0, sizeof(SolverState), st));
+  constants_kernel<<<1, 32, 0, st>>>(c64.sp);
+  count_launch();
+  prepare_kernel<double2><<<kRedBlocks, 256, 0, st>>>(diag, B, c64.n, L, c64.diag, c64.jpre, Bj);
+  prepare_kernel<float2><<<kRedBlocks, 256, 0, st>>>(diag, B, c32.n, L, c32.diag, c32.jpre, c32.vec[7]);
+  count_launch(2);
+  BDDA_CUDA_TRY(cudaGetLastError());
+  if (solver == BDDA_BICGSTAB && max_outer >= 0 && inner_tol > 0.0 && !restart) {
+    if (X0) BDDA_CUDA_TRY(cudaMemcpyAsync(X, X0, (size_t)ne * sizeof(double2), cudaMemcpyDeviceToDevice, st));
+    const int s2 = bicgstab_reliable(c64, c32, X0 != nullptr, tol, itermax, fmin(inner_tol, 0.5), iter_fin, err_fin, hist);
+    if (s2 == BDDA_OK || s2 == BDDA_NOT_CONVERGED)
+      BDDA_CUDA_TRY(cudaMemcpyAsync(Xout, X, (size_t)ne * sizeof(double2), cudaMemcpyDeviceToDevice, st));
+    return s2;
+  }
+  // ||M^-1 B||, and the first true residual
+  TRY(upd<double2>(c64, Tm, Bj, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, true));
+  norm_kernel<<<1, 256, 0, st>>>(reinterpret_cast<double*>(c64.partial), kRedBlocks, c64.st, 1);
+  count_launch();
+  if (X0) {
+    BDDA_CUDA_TRY(cudaMemcpyAsync(X, X0, (size_t)ne * sizeof(double2), cudaMemcpyDeviceToDevice, st));
+    TRY(mvp<double2>(c64, X, Tm));
+    TRY(upd<double2>(c64, R, Bj, nullptr, Tm, c64.sp.r, nullptr, nullptr, nullptr, nullptr, true));
+  } else {
+    BDDA_CUDA_TRY(cudaMemsetAsync(X, 0, (size_t)ne * sizeof(double2), st));
+    TRY(upd<double2>(c64, R, Bj, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, true));
+  }
+  norm_kernel<<<1, 256, 0, st>>>(reinterpret_cast<double*>(c64.partial), kRedBlocks, c64.st, 0);
+  count_launch();
+  double err = INFINITY;
+  int bad = 0;
+  TRY(read_state(c64, &err, &bad));
+  int total = 0;
+  *iter_fin = 0;
+  *err_fin = err;
+  int status = BDDA_NOT_CONVERGED;
+  for (int outer = 0; outer < max_outer; ++outer) {
+    if (bad == 2 || !(err == err)) { status = BDDA_NOT_CONVERGED; break; }
+    if (err < tol) { status = BDDA_OK; break; }
+    if (total >= itermax) break;
+    // inner FP32 solve of M^-1 A D = r to a relative tolerance
+    double tol_in = fmax(inner_tol, 0.3 * tol / err);
+    tol_in = fmin(tol_in, 0.5);
+    convert_in_kernel<float2><<<kRedBlocks, 256, 0, st>>>(R, c32.vec[7], ne);
+    count_launch();
+    BDDA_CUDA_TRY(cudaMemsetAsync(c32.vec[0], 0, (size_t)ne * sizeof(float2), st));
+    BDDA_CUDA_TRY(cudaMemsetAsync(c32.st, 0, sizeof(SolverState), st));
+    int it_in = 0;
+    double err_in = INFINITY;
+    const int s_in = solver == BDDA_COCG_RQ
+                         ? cocg_core<float2>(c32, false, tol_in, itermax - total, &it_in, &err_in, hist ? hist + total : nullptr)
+                         : bicgstab_core<float2>(c32, false, tol_in, itermax - total, &it_in, &err_in, hist ? hist + total : nullptr);
+    if (s_in == BDDA_BREAKDOWN) return BDDA_BREAKDOWN;
+    if (s_in != BDDA_OK && s_in != BDDA_NOT_CONVERGED) return s_in;
+    const int ran = it_in + 1;
+    if (hist)
+      for (int i = 0; i < ran; ++i) hist[total + i] *= err;   // relative to ||M^-1 B||
+    total += ran;
+    *iter_fin = total - 1;
+    if (!(err_in == err_in)) { status = BDDA_NOT_CONVERGED; break; }
+    // X += D; r = M^-1 B - M^-1 A X in FP64
+    accumulate_kernel<<<kRedBlocks, 256, 0, st>>>(X, c32.vec[0], ne);
+    count_launch();
+    TRY(mvp<double2>(c64, X, Tm));
+    TRY(upd<double2>(c64, R, Bj, nullptr, Tm, c64.sp.r, nullptr, nullptr, nullptr, nullptr, true));
+    norm_kernel<<<1, 256, 0, st>>>(reinterpret_cast<double*>(c64.partial), kRedBlocks, c64.st, 0);
+    count_launch();
+    const double prev = err;
+    TRY(read_state(c64, &err, &bad));
+    if (!(err < prev)) {   // the correction made things worse (FP32 solve past its accuracy): undo it
+      const double2 m1 = make_double2(-1.0, 0.0);
+      (void)m1;
+      negate_accumulate_kernel<<<kRedBlocks, 256, 0, st>>>(X, c32.vec[0], ne);
+      count_launch();
+      TRY(mvp<double2>(c64, X, Tm));
+      TRY(upd<double2>(c64, R, Bj, nullptr, Tm, c64.sp.r, nullptr, nullptr, nullptr, nullptr, true));
+      norm_kernel<<<1, 256, 0, st>>>(reinterpret_cast<double*>(c64.partial), kRedBlocks, c64.st, 0);
+      count_launch();
+      TRY(read_state(c64, &err, &bad));
+      *err_fin = err;
+      status = BDDA_NOT_CONVERGED;
+      break;
+    }
+    *err_fin = err;
+    if (err < tol) { status = BDDA_OK; break; }
+    if (!(err < 0.9 * prev)) { status = BDDA_NOT_CONVERGED; break; }   // refinement stalled
+  }
+  BDDA_CUDA_TRY(cudaMemcpyAsync(Xout, X, (size_t)ne * sizeof(double2), cudaMemcpyDeviceToDevice, st));
+  return status;
+}
+
 }  // namespace bdda
 
 using namespace bdda;
@@ -620,4 +897,36 @@ int bdda_cocg_rq(const bdda_plan* p, int prec, int L, int n_occ, const void* gha
                     iter_fin, err_fin, history, work, work_bytes, stream);
 }
 
+size_t bdda_refine_workspace_bytes(const bdda_plan* p, int L, int n_occ) {
+  if (!p || L < 1 || L > kMaxL || n_occ < 1) return 0;
+  return rlayout(p, L, n_occ).total;
+}
+
+int bdda_refine_solve(const bdda_plan* p, int solver, int L, int n_occ, const void* ghat_c128,
+                      const void* ghat_c64, const int32_t* cell_map, const void* diag, const void* B,
+                      const void* X0, double tol, int itermax, double inner_tol, int max_outer, void* X,
+                      int* iter_fin, double* err_fin, double* history, void* work, size_t work_bytes,
+                      void* stream) {
+  if (!p || L < 1 || L > kMaxL || n_occ < 1 || !ghat_c128 || !ghat_c64 || !cell_map || !diag || !B || !X ||
+      !iter_fin || !err_fin || itermax < 0 || max_outer == 0 || !(tol == tol) || !(inner_tol > 0.0))
+    return BDDA_BAD_ARG;
+  if (solver != BDDA_BICGSTAB && solver != BDDA_COCG_RQ) return BDDA_BAD_ARG;
+  if (!work || !p->dev_tables) return BDDA_NO_WORKSPACE;
+  *iter_fin = 0;
+  *err_fin = INFINITY;
+  if (itermax == 0) {
+    BDDA_CUDA_TRY(cudaMemsetAsync(X, 0, (size_t)3 * n_occ * L * sizeof(double2), (cudaStream_t)stream));
+    return BDDA_NOT_CONVERGED;
+  }
+  // max_outer > 0: restarted refinement; max_outer < 0 with BiCGSTAB: one FP32
+  // recursion with FP64 reliable updates (replacement factor inner_tol)
+  const bool restart = solver == BDDA_COCG_RQ || max_outer > 0;
+  if (max_outer < 0) max_outer = -max_outer;
+  return run_refine(solver, restart, p, L, n_occ, ghat_c128, ghat_c64, cell_map, static_cast<const double2*>(diag),
+                    static_cast<const double2*>(B), static_cast<const double2*>(X0), tol, itermax, inner_tol,
+                    max_outer, static_cast<double2*>(X), iter_fin, err_fin, history, work, work_bytes,
+                    (cudaStream_t)stream);
+}
+
 }  // extern "C"
+

@@ -158,6 +158,32 @@ int bdda_cocg_rq(const bdda_plan* plan, int prec, int L, int n_occ, const void* 
                  double tol, int itermax, void* X, int* iter_fin, double* err_fin,
                  double* history, void* work, size_t work_bytes, void* stream);
 
+/* ---- FP32 Krylov with FP64 refinement (no counterpart in the reference) ----------
+ * Products and Krylov vectors in complex64 (ghat_c64), the solution and the
+ * true residual r = M^-1 (B - A X) in complex128 (ghat_c128); FP64 Gram
+ * matrices and small solves.  Converged when ||r||_F / ||M^-1 B||_F < tol.
+ *  - max_outer > 0: restarted refinement, at most max_outer corrections;
+ *    each solves M^-1 A D = r in FP32 with the chosen block solver to the
+ *    relative tolerance max(inner_tol, 0.3 tol / err) and sets X += D.  A
+ *    correction that raises the true residual is undone and ends the solve.
+ *  - max_outer < 0 with BDDA_BICGSTAB: one block-BiCGSTAB recursion in FP32
+ *    with FP64 reliable updates: X accumulates in FP64 and R is replaced by
+ *    the true FP64 residual whenever the recursive residual fell by the
+ *    factor inner_tol since the last replacement and before convergence is
+ *    declared.  No restarts; suited to small L (the FP32 recursion's
+ *    attainable accuracy drops with the block width).
+ * itermax caps the FP32 iterations in total.  iter_fin = that count - 1;
+ * err_fin = the true relative residual of the returned X; history
+ * (nullable, itermax doubles) = per-iteration residual relative to
+ * ||M^-1 B||.  Returns BDDA_OK when err_fin < tol, else BDDA_NOT_CONVERGED
+ * (or BDDA_BREAKDOWN as bdda_solve). */
+size_t bdda_refine_workspace_bytes(const bdda_plan* plan, int L, int n_occ);
+int bdda_refine_solve(const bdda_plan* plan, int solver, int L, int n_occ, const void* ghat_c128,
+                      const void* ghat_c64, const int32_t* cell_map, const void* diag, const void* B,
+                      const void* X0, double tol, int itermax, double inner_tol, int max_outer, void* X,
+                      int* iter_fin, double* err_fin, double* history, void* work, size_t work_bytes,
+                      void* stream);
+
 /* ---- physics around the solve --------------------------------------------------
  * Homogeneous particle, per-axis index m_p_xyz = (re x, im x, re y, im y, re z, im z):
  * eps_r = m_p^2 / m_m^2, Clausius-Mossotti polarizability with the CR2009
@@ -185,11 +211,13 @@ int bdda_observables(int n_occ, int L, double k, double lf, int absorbing, const
 /* ---- instrumentation (no counterpart in the reference) -------------------------
  * Number of kernels this library has launched in the process.  With
  * profiling on, every block MVP records CUDA events around its five passes;
- * bdda_profile_read waits for them and returns the summed milliseconds of
- * each pass and the number of products.  Enabling clears earlier records. */
+ * bdda_profile_read waits for them and returns, over the products of one
+ * precision (prec = BDDA_C128 / BDDA_C64, or -1 for all), the summed
+ * milliseconds of each pass and the number of products.  Enabling clears
+ * earlier records. */
 unsigned long long bdda_launch_count(void);
 int bdda_profile_enable(int on);
-int bdda_profile_read(double pass_ms[5], long long* n_mvp);
+int bdda_profile_read(int prec, double pass_ms[5], long long* n_mvp);
 
 #ifdef __cplusplus
 }

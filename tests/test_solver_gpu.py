@@ -179,3 +179,37 @@ def test_specialised_block_kernels_match_generic(mods, L, solver):
         _lib.load().bdda_tune_fixed(1)
     assert err1 < 1e-6 and err2 < 1e-6 and abs(it1 - it2) <= 1
     assert rel(X1, X2) < 1e-5
+
+
+@pytest.mark.parametrize("solver", ["bicgstab", "cocg"])
+def test_mixed_precision_refinement_meets_fp64_accuracy(mods, solver):
+    """FP32 block solves inside FP64 refinement reach the true residual 1e-5 and
+    the observables agree with the FP64 solve within 1e-4 (the metric's bound)."""
+    mf, bk = mods
+    rec = load_geometry(os.path.join(GOLDEN, "geometry_cfg1.npz"))
+    n, lf, address, pos, geom, eper_r, diag, B = _case(rec)
+    til = mf.fft_init(n, 3, lf, geom["k"])
+    fn = solver_fn(bk, solver)
+    hist = []
+    Xm, itm, errm = fn(n, 3, address, til, diag, B, 1e-5, 400, precision="mixed", history=hist)
+    assert errm < 1e-5 and len(hist) == itm + 1
+    true = O.true_residual(n, 3, address, O.fft_init(n, 3, lf, geom["k"]), diag, B, Xm)
+    assert abs(true - errm) < 1e-3 * errm + 1e-9      # err_fin is the true residual
+    X64, it64, err64 = fn(n, 3, address, til, diag, B, 1e-5, 400)
+    om = O.observables(Xm, geom, pos, eper_r, lf)
+    o64 = O.observables(X64, geom, pos, eper_r, lf)
+    for key in ("C_ext", "S_fw_theta", "S_fw_phi", "S_bk"):
+        assert rel(om[key], o64[key]) < 1e-4, key
+
+
+def test_reliable_update_variant_small_block(mods):
+    """One FP32 BiCGSTAB recursion with FP64 residual replacement (L = 8)."""
+    mf, bk = mods
+    rec = load_geometry(os.path.join(GOLDEN, "geometry_cfg1.npz"))
+    n, lf, address, pos, geom, eper_r, diag, B = _case(rec)
+    til = mf.fft_init(n, 3, lf, geom["k"])
+    X, it, err = bk.bl_bicgstab_jacobi_mvp_fft(n, 3, address, til, diag, B, 1e-5, 300, precision="mixed-reliable")
+    assert err < 1e-5
+    true = O.true_residual(n, 3, address, O.fft_init(n, 3, lf, geom["k"]), diag, B, X)
+    assert abs(true - err) < 1e-3 * err + 1e-9
+    assert it + 1 <= 2 * (int(rec["bicgstab_tol5_iter_fin"]) + 1)
