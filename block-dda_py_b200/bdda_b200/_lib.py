@@ -52,6 +52,9 @@ PROTOTYPES = {
     "bdda_occupancy_map": (_i, [_vp, _vp, _i, _vp, _vp]),
     "bdda_fft_mvp": (_i, [_vp, _i, _i, _vp, _vp, _vp, _vp, _vp]),
     "bdda_block_mvp": (_i, [_vp, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "bdda_block_mvp_noalloc_max_bytes": (_sz, []),
+    "bdda_block_mvp_noalloc_fits": (_i, [_vp, _i, _i]),
+    "bdda_block_mvp_noalloc": (_i, [_vp, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "bdda_solver_workspace_bytes": (_sz, [_vp, _i, _i, _i, _i]),
     "bdda_refine_workspace_bytes": (_sz, [_vp, _i, _i]),
     "bdda_refine_solve": (_i, [_vp, _i, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _d, _i, _d, _i, _vp, _pi,

@@ -127,6 +127,26 @@ int bdda_block_mvp(const bdda_plan* plan, int prec, int L, const void* ghat,
                    const int32_t* cell_map, const void* diag, const void* jpre, const void* S,
                    void* out, void* work, void* stream);
 
+/* Block MVP with no scratch argument (no counterpart in the reference).  For
+ * callers that cannot allocate device memory -- a plugin whose host
+ * application's allocator owns all device memory, or a latency-critical path
+ * that cannot take the synchronisation cudaMalloc / cudaFree may imply.  Same
+ * product and arguments as bdda_block_mvp minus `work`; the scratch field
+ * buffer is a static 64 MiB device array (bdda_block_mvp_noalloc_max_bytes())
+ * that every GPU loading the library holds until exit.  Returns BDDA_BAD_ARG
+ * when bdda_mvp_workspace_bytes(plan, prec, L) exceeds it
+ * (bdda_block_mvp_noalloc_fits() tells in advance).  All calls on a device
+ * share the array: calls that overlap on the GPU race, so serialise them.
+ * Nothing in it needs to start at zero.  The first call on a device looks up
+ * the array's address with that device current; make it before any stream
+ * capture.  It allocates nothing (cudaMalloc, cudaFree and allocating library
+ * routines are never called; profiling, off by default, creates CUDA events). */
+size_t bdda_block_mvp_noalloc_max_bytes(void);
+int bdda_block_mvp_noalloc_fits(const bdda_plan* plan, int prec, int L);
+int bdda_block_mvp_noalloc(const bdda_plan* plan, int prec, int L, const void* ghat,
+                           const int32_t* cell_map, const void* diag, const void* jpre, const void* S,
+                           void* out, void* stream);
+
 /* ---- block Krylov solvers -----------------------------------------------------
  * Solve A X = B with Jacobi left preconditioning, M = diag(A): iterate on
  * M^-1 A X = M^-1 B until ||R||_F / ||M^-1 B||_F < tol (a single global
