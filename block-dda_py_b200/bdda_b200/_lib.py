@@ -26,6 +26,7 @@ _sz = C.c_size_t
 _i = C.c_int
 _d = C.c_double
 _pi = C.POINTER(C.c_int)
+_pd = C.POINTER(C.c_double)
 
 # name -> (restype, argtypes).  Every symbol of include/bdda.h is listed here;
 # tests check the two lists against each other.
@@ -35,6 +36,9 @@ PROTOTYPES = {
     "bdda_tune_set": (_i, [_i, _i, _sz, _i]),
     "bdda_tune_get": (_i, [_i, _i, C.POINTER(_sz), _pi]),
     "bdda_tune_fixed": (_i, [_i]),
+    "bdda_tune_pass": (_i, [_i, _i, _i, _i, _i, _i]),
+    "bdda_tune_pass_get": (_i, [_i, _i, _i, _i, _pi, _pi]),
+    "bdda_autotune": (_i, [_vp, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i, _pd, _pd, _vp]),
     "bdda_plan_create": (_i, [_pi, _pi, C.POINTER(_vp)]),
     "bdda_plan_destroy": (None, [_vp]),
     "bdda_plan_grid": (_i, [_vp, _pi]),

@@ -205,3 +205,29 @@ class Occupancy:
         _lib.check(_lib.load().bdda_occupancy_map(plan.handle, ptr(self.address_dev), self.n_occ,
                                                   ptr(self.cell_map), stream_ptr(plan.device)),
                    "bdda_occupancy_map")
+
+
+def autotune(green: GreenTensor, occupancy: Occupancy, L: int, precision="c128", reps: int = 3,
+             seed: int = 0) -> tuple[float, float]:
+    """Pick each pencil pass's tile width and kernel variant for this grid and L.
+
+    Runs block MVPs on random input (libbdda's ``bdda_autotune``), keeps the
+    fastest launch choice per pass, and returns the product's time in ms
+    before and after.  The choice is process-wide and applies to every later
+    product with the same axis lengths, precision and L.
+    """
+    prec = precision_code(precision)
+    plan = green.plan
+    dev = plan.device
+    dt = TORCH_DTYPE[prec]
+    n3 = 3 * occupancy.n_occ
+    g = torch.Generator(device=dev).manual_seed(int(seed))
+    S = torch.randn((n3, int(L)), dtype=dt, device=dev, generator=g)
+    diag = torch.ones(n3, dtype=dt, device=dev)
+    out = torch.empty_like(S)
+    before, after = C.c_double(), C.c_double()
+    _lib.check(_lib.load().bdda_autotune(plan.handle, prec, int(L), ptr(green.ghat(prec)), ptr(occupancy.cell_map),
+                                         ptr(diag), ptr(diag), ptr(S), ptr(out), ptr(green.workspace(prec, L)),
+                                         int(reps), C.byref(before), C.byref(after), stream_ptr(dev)),
+               "bdda_autotune")
+    return before.value, after.value

@@ -53,14 +53,18 @@ __device__ __forceinline__ void fixed_mid(const PassArgs& a, const Pen& c, T* sm
   }
 }
 
-template <typename T, int KIND, int LT, int NT, int R0, int R1, int R2, int R3>
-__global__ void __launch_bounds__(NT) fixed_pencil_kernel(const PassArgs a) {
+// MINB: resident CTAs per SM the register allocation must allow (the
+// __launch_bounds__ minimum); 1 = no bound.  complex128 kernels are compiled
+// with 3 and 4 and the autotuner picks per pass.
+template <typename T, int KIND, int LT, int NT, int MINB, int R0, int R1, int R2, int R3>
+__global__ void __launch_bounds__(NT, MINB) fixed_pencil_kernel(const PassArgs a) {
   using RS = RadixSeq<R0, R1, R2, R3>;
   constexpr int N = RS::n;
   extern __shared__ __align__(16) unsigned char smraw[];
   T *tw, *sm, *gs;
-  stage_constants<T, KIND, LT>(a, smraw, RS::M, &tw, &sm, &gs);
-  const Pen c = pen_of_block(a);
+  int32_t* cm;
+  stage_constants<T, KIND, LT>(a, smraw, RS::M, &tw, &sm, &gs, &cm);
+  const Pen c = pen_of_block<T>(a, cm);
   if constexpr (KIND == K_FWD) {
     if constexpr (N == 1) {
       fixed_stage<RS, 0, false, 1, 1, KIND, T, LT, NT>(a, c, sm, tw);
@@ -100,14 +104,14 @@ __global__ void __launch_bounds__(NT) fixed_pencil_kernel(const PassArgs a) {
   }
 }
 
-template <typename T, int KIND, int LT, int R0, int R1, int R2, int R3>
+template <typename T, int KIND, int LT, int MINB, int R0, int R1, int R2, int R3>
 int fixed_launch(const PassArgs& a0, int64_t P0, cudaStream_t st) {
   constexpr int NT = 256;
   using RS = RadixSeq<R0, R1, R2, R3>;
   PassArgs a = a0;
   if (a.ax.M != RS::M) return BDDA_BAD_ARG;
   a.ntile = (a.L + LT - 1) / LT;
-  auto kern = fixed_pencil_kernel<T, KIND, LT, NT, R0, R1, R2, R3>;
+  auto kern = fixed_pencil_kernel<T, KIND, LT, NT, MINB, R0, R1, R2, R3>;
   const size_t smem = (size_t)pencil_smem_bytes<T>(RS::M, LT, KIND);
   if (smem > 227 * 1024) return BDDA_BAD_ARG;
   const int64_t nblk = P0 * a.P1 * a.ntile;
@@ -120,7 +124,7 @@ int fixed_launch(const PassArgs& a0, int64_t P0, cudaStream_t st) {
   return BDDA_OK;
 }
 
-#define BDDA_FIXED(T, PREC, KIND, LT, R0, R1, R2, R3) \
-  { PREC, KIND, LT, {R0, R1, R2, R3}, &fixed_launch<T, KIND, LT, R0, R1, R2, R3> }
+#define BDDA_FIXED(T, PREC, KIND, LT, MINB, R0, R1, R2, R3) \
+  { PREC, KIND, LT, MINB, {R0, R1, R2, R3}, &fixed_launch<T, KIND, LT, MINB, R0, R1, R2, R3> }
 
 }  // namespace bdda

@@ -7,14 +7,14 @@
 namespace bdda {
 
 static const FixedKernel kTableB[] = {
-    BDDA_FIXED(float2, 1, K_CONV, 8, 8, 8, 3, 1),
-    BDDA_FIXED(float2, 1, K_FWD, 8, 8, 7, 4, 1),
-    BDDA_FIXED(float2, 1, K_INV, 8, 8, 7, 4, 1),
-    BDDA_FIXED(float2, 1, K_FWD, 8, 10, 7, 5, 1),
-    BDDA_FIXED(float2, 1, K_INV, 8, 10, 7, 5, 1),
-    BDDA_FIXED(float2, 1, K_CONV, 8, 7, 4, 2, 1),
-    BDDA_FIXED(float2, 1, K_FWD, 8, 8, 7, 1, 1),
-    BDDA_FIXED(float2, 1, K_INV, 8, 8, 7, 1, 1),
+    BDDA_FIXED(float2, 1, K_CONV, 8, 1, 8, 8, 3, 1),
+    BDDA_FIXED(float2, 1, K_FWD, 8, 1, 8, 7, 4, 1),
+    BDDA_FIXED(float2, 1, K_INV, 8, 1, 8, 7, 4, 1),
+    BDDA_FIXED(float2, 1, K_FWD, 8, 1, 10, 7, 5, 1),
+    BDDA_FIXED(float2, 1, K_INV, 8, 1, 10, 7, 5, 1),
+    BDDA_FIXED(float2, 1, K_CONV, 8, 1, 7, 4, 2, 1),
+    BDDA_FIXED(float2, 1, K_FWD, 8, 1, 8, 7, 1, 1),
+    BDDA_FIXED(float2, 1, K_INV, 8, 1, 8, 7, 1, 1),
 };
 
 const FixedKernel* fixed_table_b(int* n) {

@@ -15,6 +15,7 @@
 #include <cstring>
 #include <type_traits>
 #include <algorithm>
+#include <mutex>
 #include <vector>
 
 #include "bdda_internal.h"
@@ -32,8 +33,9 @@ __global__ void __launch_bounds__(256) pencil_kernel(const PassArgs a) {
   extern __shared__ __align__(16) unsigned char smraw[];
   const int M = a.ax.M, nst = a.ax.nst;
   T *tw, *sm, *gs;
-  stage_constants<T, KIND, LT>(a, smraw, M, &tw, &sm, &gs);
-  const Pen c = pen_of_block(a);
+  int32_t* cm;
+  stage_constants<T, KIND, LT>(a, smraw, M, &tw, &sm, &gs, &cm);
+  const Pen c = pen_of_block<T>(a, cm);
   if constexpr (KIND == K_FWD) {
     bool staged = false;
     if constexpr (std::is_same<T, double2>::value) {
@@ -100,13 +102,38 @@ static size_t pencil_smem(int M, int LT, int kind) {
 // Launch shape of the pencil passes, per precision (0 c128, 1 c64) and pass
 // kind: the shared-memory budget per CTA (the widest column tile that fits is
 // used) and the threads per CTA.  Set by bdda_tune_set.
-static size_t g_tile_smem_budget[2][3] = {{72 * 1024, 72 * 1024, 72 * 1024},
-                                          {72 * 1024, 72 * 1024, 72 * 1024}};
+static size_t g_tile_smem_budget[2][3] = {{80 * 1024, 80 * 1024, 80 * 1024},
+                                          {80 * 1024, 80 * 1024, 80 * 1024}};
 static int g_threads[2][3] = {{256, 256, 256}, {256, 256, 256}};
 static_assert(K_FWD == 0 && K_CONV == 1 && K_INV == 2, "tuning tables are indexed by pass kind");
 
+// Per-pass launch choices set by the autotuner (bdda_tune_pass), keyed by
+// precision, pass kind, axis length and L: the column tile width lt (0 = the
+// shared-memory budget rule) and the kernel variant (0 = the first
+// specialised kernel compiled, k > 0 = the one compiled for k resident CTAs
+// per SM, -1 = the generic kernel).
+struct PassTune { int prec, kind, M, L, lt, variant; };
+static std::vector<PassTune> g_pass_tune;
+static std::mutex g_tune_mu;
+
+static PassTune pass_tune(int prec, int kind, int M, int L) {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  for (const auto& e : g_pass_tune)
+    if (e.prec == prec && e.kind == kind && e.M == M && e.L == L) return e;
+  return PassTune{prec, kind, M, L, 0, 0};
+}
+
+static void set_pass_tune(const PassTune& t) {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  for (auto& e : g_pass_tune)
+    if (e.prec == t.prec && e.kind == t.kind && e.M == t.M && e.L == t.L) { e = t; return; }
+  g_pass_tune.push_back(t);
+}
+
 template <typename T>
 static int pick_lt(int M, int L, int kind) {
+  const PassTune t = pass_tune(prec_of<T>(), kind, M, L);
+  if (t.lt > 0 && pencil_smem<T>(M, t.lt, kind) <= 227 * 1024) return t.lt;
   const int cand[3] = {8, 4, 2};
   for (int lt : cand) {
     if (lt > 2 && lt / 2 >= L) continue;
@@ -133,8 +160,32 @@ static int launch_lt(PassArgs a, int64_t P0, cudaStream_t st) {
 
 static int g_use_fixed = 1;   // specialised kernels on (bdda_tune_fixed)
 
-static FixedLaunchFn fixed_find(int prec, int kind, int lt, const AxisFFT& ax) {
-  if (!g_use_fixed || ax.nst > 4) return nullptr;
+// Specialised kernel for (precision, kind, tile width, radix sequence);
+// variant as in PassTune.
+static FixedLaunchFn fixed_find(int prec, int kind, int lt, const AxisFFT& ax, int variant) {
+  if (!g_use_fixed || variant < 0 || ax.nst > 4) return nullptr;
+  int r[4] = {1, 1, 1, 1};
+  for (int s = 0; s < ax.nst; ++s) r[s] = ax.rad[s];
+  FixedLaunchFn first = nullptr;
+  for (int t = 0; t < 2; ++t) {
+    int n = 0;
+    const FixedKernel* tab = t == 0 ? fixed_table_a(&n) : fixed_table_b(&n);
+    for (int i = 0; i < n; ++i) {
+      const FixedKernel& f = tab[i];
+      if (f.prec == prec && f.kind == kind && f.lt == lt && f.r[0] == r[0] && f.r[1] == r[1] &&
+          f.r[2] == r[2] && f.r[3] == r[3]) {
+        if (variant == 0 || f.minb == variant) return f.fn;
+        if (!first) first = f.fn;
+      }
+    }
+  }
+  return first;
+}
+
+// Register-bound variants compiled for (precision, kind, tile width, radix sequence).
+static std::vector<int> fixed_variants(int prec, int kind, int lt, const AxisFFT& ax) {
+  std::vector<int> out;
+  if (ax.nst > 4) return out;
   int r[4] = {1, 1, 1, 1};
   for (int s = 0; s < ax.nst; ++s) r[s] = ax.rad[s];
   for (int t = 0; t < 2; ++t) {
@@ -144,16 +195,17 @@ static FixedLaunchFn fixed_find(int prec, int kind, int lt, const AxisFFT& ax) {
       const FixedKernel& f = tab[i];
       if (f.prec == prec && f.kind == kind && f.lt == lt && f.r[0] == r[0] && f.r[1] == r[1] &&
           f.r[2] == r[2] && f.r[3] == r[3])
-        return f.fn;
+        out.push_back(f.minb);
     }
   }
-  return nullptr;
+  return out;
 }
 
 template <typename T, int KIND>
 static int launch_pass(const PassArgs& a, int64_t P0, int lt, cudaStream_t st) {
   if (!a.green) {
-    FixedLaunchFn f = fixed_find(prec_of<T>(), KIND, lt, a.ax);
+    const int variant = pass_tune(prec_of<T>(), KIND, a.ax.M, a.L).variant;
+    FixedLaunchFn f = fixed_find(prec_of<T>(), KIND, lt, a.ax, variant);
     if (f) return f(a, P0, st);
   }
   switch (lt) {
@@ -177,7 +229,8 @@ template <> struct TwOff<float2> { static size_t get(const bdda_plan* p, int ax)
 // (fft_mvp); otherwise the sparse block MVP with diagonal and Jacobi scaling.
 template <typename T>
 static int run_mvp(const bdda_plan* plan, int L, const T* ghat, const int32_t* cell_map,
-                   const T* src, const T* diag, const T* jpre, T* out, T* F, cudaStream_t st) {
+                   const T* src, const T* diag, const T* jpre, T* out, T* F, cudaStream_t st,
+                   cudaEvent_t* ev = nullptr) {
   const int64_t Nx = plan->n[0], Ny = plan->n[1], Nz = plan->n[2];
   const int64_t Mx = plan->ax[0].M, My = plan->ax[1].M, Mz = plan->ax[2].M;
   const int64_t C = 3 * (int64_t)L;
@@ -188,6 +241,7 @@ static int run_mvp(const bdda_plan* plan, int L, const T* ghat, const int32_t* c
   b.scale = 1.0;
   const bool prof = profiling();
   if (prof) profile_mark(0, st, prec_of<T>());
+  if (ev) BDDA_CUDA_TRY(cudaEventRecord(ev[0], st));
 
   {  // Z: gather + forward z
     PassArgs a = b;
@@ -199,6 +253,7 @@ static int run_mvp(const bdda_plan* plan, int L, const T* ghat, const int32_t* c
     a.dst = F; a.dst_p0 = My * Mz * C; a.dst_p1 = Mz * C; a.dst_row = C;
     BDDA_TRY((launch_pass<T, K_FWD>(a, Nx, pick_lt<T>((int)Mz, L, K_FWD), st)));
     if (prof) profile_mark(1, st);
+    if (ev) BDDA_CUDA_TRY(cudaEventRecord(ev[1], st));
   }
   PassArgs ay = b;  // Y and Y^-1 share the pencil geometry
   ay.ax = plan->ax[1]; ay.tw = table_ptr<T>(plan, TwOff<T>::get(plan, 1));
@@ -209,6 +264,7 @@ static int run_mvp(const bdda_plan* plan, int L, const T* ghat, const int32_t* c
     a.n_in = (int)Ny; a.n_out = (int)My;
     BDDA_TRY((launch_pass<T, K_FWD>(a, Nx, pick_lt<T>((int)My, L, K_FWD), st)));
     if (prof) profile_mark(2, st);
+    if (ev) BDDA_CUDA_TRY(cudaEventRecord(ev[2], st));
   }
   {  // X: forward, Green multiply, inverse
     PassArgs a = b;
@@ -219,12 +275,14 @@ static int run_mvp(const bdda_plan* plan, int L, const T* ghat, const int32_t* c
     a.ghat = ghat;
     BDDA_TRY((launch_pass<T, K_CONV>(a, My, pick_lt<T>((int)Mx, L, K_CONV), st)));
     if (prof) profile_mark(3, st);
+    if (ev) BDDA_CUDA_TRY(cudaEventRecord(ev[3], st));
   }
   {
     PassArgs a = ay;
     a.n_in = (int)My; a.n_out = (int)Ny;
     BDDA_TRY((launch_pass<T, K_INV>(a, Nx, pick_lt<T>((int)My, L, K_INV), st)));
     if (prof) profile_mark(4, st);
+    if (ev) BDDA_CUDA_TRY(cudaEventRecord(ev[4], st));
   }
   {  // Z^-1 + crop + epilogue
     PassArgs a = b;
@@ -237,6 +295,7 @@ static int run_mvp(const bdda_plan* plan, int L, const T* ghat, const int32_t* c
     a.scale = 1.0 / (double)(Mx * My * Mz);
     BDDA_TRY((launch_pass<T, K_INV>(a, Nx, pick_lt<T>((int)Mz, L, K_INV), st)));
     if (prof) profile_mark(5, st);
+    if (ev) BDDA_CUDA_TRY(cudaEventRecord(ev[5], st));
   }
   return BDDA_OK;
 }
@@ -252,6 +311,91 @@ template int block_mvp_impl<double2>(const bdda_plan*, int, const double2*, cons
 template int block_mvp_impl<float2>(const bdda_plan*, int, const float2*, const int32_t*,
                                     const float2*, const float2*, const float2*, float2*, float2*,
                                     cudaStream_t);
+
+// ---- autotuner -----------------------------------------------------------------
+// Times every launch choice of each pass of one block MVP (tile width x
+// kernel variant) on the caller's buffers and keeps the fastest per
+// (precision, kind, axis length, L).  All passes advance through their
+// candidate lists together, one block MVP per round, each pass timed by its
+// own pair of events; passes that share a key add their times.
+template <typename T>
+static int autotune_impl(const bdda_plan* p, int L, const T* ghat, const int32_t* cmap, const T* diag,
+                         const T* jpre, const T* S, T* out, T* work, cudaStream_t st, int reps,
+                         double* ms_before, double* ms_after) {
+  const int prec = prec_of<T>();
+  const int pass_kind[5] = {K_FWD, K_FWD, K_CONV, K_INV, K_INV};
+  const int pass_axis[5] = {2, 1, 0, 1, 2};
+  struct Key {
+    int kind, axis;
+    std::vector<PassTune> cand;
+    std::vector<double> ms;
+  };
+  std::vector<Key> keys;
+  int key_of[5];
+  for (int q = 0; q < 5; ++q) {
+    const int M = p->ax[pass_axis[q]].M;
+    int k = -1;
+    for (size_t i = 0; i < keys.size(); ++i)
+      if (keys[i].kind == pass_kind[q] && p->ax[keys[i].axis].M == M) k = (int)i;
+    if (k < 0) {
+      Key key;
+      key.kind = pass_kind[q];
+      key.axis = pass_axis[q];
+      for (int lt : {8, 4, 2}) {
+        if (lt > 2 && lt / 2 >= L) continue;
+        if (pencil_smem<T>(M, lt, key.kind) > 227 * 1024) continue;
+        for (int v : fixed_variants(prec, key.kind, lt, p->ax[key.axis])) key.cand.push_back({prec, key.kind, M, L, lt, v});
+        key.cand.push_back({prec, key.kind, M, L, lt, -1});
+      }
+      key.ms.assign(key.cand.size(), 0.0);
+      keys.push_back(key);
+      k = (int)keys.size() - 1;
+    }
+    key_of[q] = k;
+  }
+  size_t rounds = 0;
+  for (const auto& k : keys) rounds = std::max(rounds, k.cand.size());
+  std::vector<cudaEvent_t> ev(6);
+  for (auto& e : ev) BDDA_CUDA_TRY(cudaEventCreate(&e));
+  auto timed = [&](double pass_ms[5]) -> int {
+    for (int q = 0; q < 5; ++q) pass_ms[q] = 0.0;
+    BDDA_TRY(run_mvp<T>(p, L, ghat, cmap, S, diag, jpre, out, work, st));   // warm-up
+    for (int r = 0; r < reps; ++r) {
+      BDDA_TRY(run_mvp<T>(p, L, ghat, cmap, S, diag, jpre, out, work, st, ev.data()));
+      BDDA_CUDA_TRY(cudaEventSynchronize(ev[5]));
+      for (int q = 0; q < 5; ++q) {
+        float ms = 0.f;
+        BDDA_CUDA_TRY(cudaEventElapsedTime(&ms, ev[q], ev[q + 1]));
+        pass_ms[q] += ms / reps;
+      }
+    }
+    return BDDA_OK;
+  };
+  double pm[5];
+  int status = timed(pm);
+  if (status == BDDA_OK && ms_before) *ms_before = pm[0] + pm[1] + pm[2] + pm[3] + pm[4];
+  for (size_t r = 0; r < rounds && status == BDDA_OK; ++r) {
+    for (auto& k : keys) set_pass_tune(k.cand[std::min(r, k.cand.size() - 1)]);
+    status = timed(pm);
+    for (int q = 0; q < 5 && status == BDDA_OK; ++q) {
+      Key& k = keys[key_of[q]];
+      if (r < k.cand.size()) k.ms[r] += pm[q];
+    }
+  }
+  for (auto& k : keys) {
+    if (k.cand.empty()) continue;
+    size_t b = 0;
+    for (size_t i = 1; i < k.ms.size(); ++i)
+      if (k.ms[i] < k.ms[b]) b = i;
+    set_pass_tune(k.cand[b]);
+  }
+  if (status == BDDA_OK) {
+    status = timed(pm);
+    if (status == BDDA_OK && ms_after) *ms_after = pm[0] + pm[1] + pm[2] + pm[3] + pm[4];
+  }
+  for (auto& e : ev) cudaEventDestroy(e);
+  return status;
+}
 
 // ---- small helper kernels ----------------------------------------------------
 __global__ void occupancy_kernel(const int64_t* address, int n_occ, int64_t nc, int32_t* cell_map) {
@@ -422,6 +566,42 @@ int bdda_tune_set(int prec, int kind, size_t smem_budget, int threads) {
   g_tile_smem_budget[prec][kind] = smem_budget;
   g_threads[prec][kind] = threads;
   return BDDA_OK;
+}
+
+int bdda_tune_pass(int prec, int kind, int M, int L, int lt, int variant) {
+  if (prec < 0 || prec > 1 || kind < 0 || kind > 2 || M < 1 || L < 1 || L > kMaxL ||
+      (lt != 0 && lt != 2 && lt != 4 && lt != 8) || variant < -1 || variant > 8)
+    return BDDA_BAD_ARG;
+  set_pass_tune({prec, kind, M, L, lt, variant});
+  return BDDA_OK;
+}
+
+int bdda_tune_pass_get(int prec, int kind, int M, int L, int* lt, int* variant) {
+  if (!lt || !variant) return BDDA_BAD_ARG;
+  const PassTune t = pass_tune(prec, kind, M, L);
+  *lt = t.lt;
+  *variant = t.variant;
+  return BDDA_OK;
+}
+
+int bdda_autotune(const bdda_plan* plan, int prec, int L, const void* ghat, const int32_t* cell_map,
+                  const void* diag, const void* jpre, const void* S, void* out, void* work, int reps,
+                  double* ms_before, double* ms_after, void* stream) {
+  if (!plan || L < 1 || L > kMaxL || reps < 1 || !ghat || !cell_map || !diag || !jpre || !S || !out)
+    return BDDA_BAD_ARG;
+  if (!plan->dev_tables || !work) return BDDA_NO_WORKSPACE;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (prec == BDDA_C128)
+    return autotune_impl<double2>(plan, L, static_cast<const double2*>(ghat), cell_map,
+                                  static_cast<const double2*>(diag), static_cast<const double2*>(jpre),
+                                  static_cast<const double2*>(S), static_cast<double2*>(out),
+                                  static_cast<double2*>(work), st, reps, ms_before, ms_after);
+  if (prec == BDDA_C64)
+    return autotune_impl<float2>(plan, L, static_cast<const float2*>(ghat), cell_map,
+                                 static_cast<const float2*>(diag), static_cast<const float2*>(jpre),
+                                 static_cast<const float2*>(S), static_cast<float2*>(out),
+                                 static_cast<float2*>(work), st, reps, ms_before, ms_after);
+  return BDDA_BAD_ARG;
 }
 
 int bdda_tune_fixed(int on) {

@@ -46,6 +46,9 @@ struct PassArgs {
 struct Pen {
   int64_t p0, p1;
   int tile;
+  const void* srcb;      // pencil base of the source: src + p0 src_p0 + p1 src_p1
+  void* dstb;            // pencil base of the destination
+  const int32_t* cmap;   // this pencil's occupancy-map entries, staged in shared memory (or null)
 };
 
 __device__ __forceinline__ bool axis_disp(int I, int N, int M, int& d) {
@@ -110,16 +113,20 @@ template <typename T> constexpr int prec_of() { return std::is_same<T, double2>:
 template <typename T>
 __host__ __device__ __forceinline__ int pencil_smem_bytes(int M, int LT, int kind) {
   return align16(M * (int)sizeof(T)) + align16(M * 3 * LT * (int)sizeof(T)) +
-         (kind == K_CONV ? align16(M * 6 * (int)sizeof(T)) : 0);
+         (kind == K_CONV ? align16(M * 6 * (int)sizeof(T)) : 0) + align16(M * 4);
 }
 
 // Pencil and tile of a CTA (one item per CTA).
-__device__ __forceinline__ Pen pen_of_block(const PassArgs& a) {
+template <typename T>
+__device__ __forceinline__ Pen pen_of_block(const PassArgs& a, const int32_t* cm) {
   Pen c;
   c.tile = (int)(blockIdx.x % a.ntile);
   const int64_t p = blockIdx.x / a.ntile;
   c.p0 = p / a.P1;
   c.p1 = p - c.p0 * a.P1;
+  c.srcb = static_cast<const T*>(a.src) + c.p0 * a.src_p0 + c.p1 * a.src_p1;
+  c.dstb = static_cast<T*>(a.dst) + c.p0 * a.dst_p0 + c.p1 * a.dst_p1;
+  c.cmap = a.cell_map ? cm : nullptr;
   return c;
 }
 
@@ -127,10 +134,14 @@ __device__ __forceinline__ Pen pen_of_block(const PassArgs& a) {
 // for the X pass, the Green's pencil).  Returns after the twiddles landed.
 template <typename T, int KIND, int LT>
 __device__ __forceinline__ void stage_constants(const PassArgs& a, unsigned char* smraw, int M, T** tw, T** sm,
-                                                T** gs) {
+                                                T** gs, int32_t** cm) {
+  const int o_sm = align16(M * (int)sizeof(T));
+  const int o_gs = o_sm + align16(M * 3 * LT * (int)sizeof(T));
+  const int o_cm = o_gs + (KIND == K_CONV ? align16(M * 6 * (int)sizeof(T)) : 0);
   *tw = reinterpret_cast<T*>(smraw);
-  *sm = reinterpret_cast<T*>(smraw + align16(M * (int)sizeof(T)));
-  *gs = reinterpret_cast<T*>(smraw + align16(M * (int)sizeof(T)) + align16(M * 3 * LT * (int)sizeof(T)));
+  *sm = reinterpret_cast<T*>(smraw + o_sm);
+  *gs = reinterpret_cast<T*>(smraw + o_gs);
+  *cm = reinterpret_cast<int32_t*>(smraw + o_cm);
   async_copy(*tw, a.tw, M * (int)sizeof(T));
   cp_async_commit();
   if constexpr (KIND == K_CONV) {
@@ -138,6 +149,13 @@ __device__ __forceinline__ void stage_constants(const PassArgs& a, unsigned char
     async_copy(*gs, static_cast<const T*>(a.ghat) + p * (int64_t)M * 6, M * 6 * (int)sizeof(T));
   }
   cp_async_commit();
+  if (a.cell_map) {   // the pencil's occupancy-map rows (Z and Z^-1 passes)
+    const int64_t p = blockIdx.x / a.ntile;
+    const int64_t p0 = p / a.P1, p1 = p - p0 * a.P1;
+    const int32_t* src = a.cell_map + p0 * a.cell_p0 + p1 * a.cell_p1;
+    const int rows = KIND == K_INV ? a.n_out : a.n_in;
+    for (int i = threadIdx.x; i < rows; i += blockDim.x) (*cm)[i] = src[i];
+  }
   cp_async_wait<1>();
   __syncthreads();
 }
@@ -145,32 +163,42 @@ __device__ __forceinline__ void stage_constants(const PassArgs& a, unsigned char
 
 
 // ---- global row access of one pencil x column tile ----
+// Column col of the tile is right-hand side tile*LT + col%LT of component
+// col/LT, i.e. grid column (col/LT)*L + tile*LT + col%LT.
+template <int LT>
+__device__ __forceinline__ int tile_gcol(const PassArgs& a, const Pen& c, int col, bool& ok) {
+  const int comp = col / LT, l = c.tile * LT + (col - comp * LT);
+  ok = l < a.L;
+  return comp * a.L + l;
+}
+
 template <int KIND, typename T, int LT>
 __device__ __forceinline__ T gload(const PassArgs& a, const Pen& c, int row, int col) {
   typedef typename real_of<T>::type F;
-  const int comp = col / LT, l = c.tile * LT + (col - comp * LT);
-  if (row >= a.n_in || l >= a.L) return mkc<T>(F(0), F(0));
-  const int64_t gcol = (int64_t)comp * a.L + l;
+  bool ok;
+  const int gcol = tile_gcol<LT>(a, c, col, ok);
+  if (!ok || row >= a.n_in) return mkc<T>(F(0), F(0));
   if constexpr (KIND == K_FWD) {
-    if (a.cell_map) {
-      const int m = a.cell_map[c.p0 * a.cell_p0 + c.p1 * a.cell_p1 + row];
+    if (c.cmap) {
+      const int m = c.cmap[row];
       return m >= 0 ? static_cast<const T*>(a.S)[(int64_t)m * a.C + gcol] : mkc<T>(F(0), F(0));
     }
   }
-  return static_cast<const T*>(a.src)[c.p0 * a.src_p0 + c.p1 * a.src_p1 + (int64_t)row * a.src_row + gcol];
+  return static_cast<const T*>(c.srcb)[(int64_t)row * a.src_row + gcol];
 }
 
 template <int KIND, typename T, int LT>
 __device__ __forceinline__ void gstore(const PassArgs& a, const Pen& c, int row, int col, T v) {
   typedef typename real_of<T>::type F;
-  const int comp = col / LT, l = c.tile * LT + (col - comp * LT);
-  if (row >= a.n_out || l >= a.L) return;
-  const int64_t gcol = (int64_t)comp * a.L + l;
+  bool ok;
+  const int gcol = tile_gcol<LT>(a, c, col, ok);
+  if (!ok || row >= a.n_out) return;
   if constexpr (KIND == K_INV) {
     const F sc = F(a.scale);
-    if (a.cell_map) {   // crop + gather + diagonal + Jacobi: (diag S + y) jpre (bl_krylov.py:55)
-      const int m = a.cell_map[c.p0 * a.cell_p0 + c.p1 * a.cell_p1 + row];
+    if (c.cmap) {   // crop + gather + diagonal + Jacobi: (diag S + y) jpre (bl_krylov.py:55)
+      const int m = c.cmap[row];
       if (m >= 0) {
+        const int comp = col / LT;
         const int64_t r3 = 3 * (int64_t)m + comp;
         const int64_t idx = (int64_t)m * a.C + gcol;
         const T d = static_cast<const T*>(a.diag)[r3];
@@ -182,7 +210,7 @@ __device__ __forceinline__ void gstore(const PassArgs& a, const Pen& c, int row,
     }
     v = cscale(v, sc);
   }
-  static_cast<T*>(a.dst)[c.p0 * a.dst_p0 + c.p1 * a.dst_p1 + (int64_t)row * a.dst_row + gcol] = v;
+  static_cast<T*>(c.dstb)[(int64_t)row * a.dst_row + gcol] = v;
 }
 
 // ---- one radix-R butterfly of a stage; rows base + q*span of column col ----
@@ -319,6 +347,7 @@ __device__ void run_conv_mid(const PassArgs& a, const Pen& c, T* sm, const T* gs
 typedef int (*FixedLaunchFn)(const PassArgs& a, int64_t P0, cudaStream_t st);
 struct FixedKernel {
   int prec, kind, lt;
+  int minb;            // register bound: resident CTAs per SM (1 = none)
   int r[4];            // radix sequence, padded with 1
   FixedLaunchFn fn;
 };

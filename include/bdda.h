@@ -87,6 +87,23 @@ int bdda_plan_attach_tables(bdda_plan* plan, void* dev_tables, void* stream);
  * threads per CTA is a multiple of 32 up to 512.  Process-wide settings. */
 int bdda_tune_set(int prec, int kind, size_t smem_budget, int threads);
 int bdda_tune_get(int prec, int kind, size_t* smem_budget, int* threads);
+/* Per-pass launch choice for passes of (prec, kind) over an axis of length M
+ * at block width L: column tile width lt (2, 4, 8; 0 = the smem_budget rule)
+ * and kernel variant (0 = the first specialised kernel compiled for the radix
+ * sequence, k > 0 = the one compiled for k resident CTAs per SM, -1 = the
+ * generic run-time-radix kernel).  Process-wide; set by bdda_autotune. */
+int bdda_tune_pass(int prec, int kind, int M, int L, int lt, int variant);
+int bdda_tune_pass_get(int prec, int kind, int M, int L, int* lt, int* variant);
+/* Autotuner (no counterpart in the reference; the reference's scipy.fft plans
+ * itself).  Runs block MVPs of this plan on the caller's buffers (arguments as
+ * bdda_block_mvp; out and work are overwritten), times each pass over every
+ * candidate (tile width x kernel variant) with CUDA events, reps timed
+ * products per candidate, and keeps the fastest per pass key through
+ * bdda_tune_pass.  ms_before / ms_after (nullable): one product before and
+ * after.  Synchronises the stream; do not call during stream capture. */
+int bdda_autotune(const bdda_plan* plan, int prec, int L, const void* ghat, const int32_t* cell_map,
+                  const void* diag, const void* jpre, const void* S, void* out, void* work, int reps,
+                  double* ms_before, double* ms_after, void* stream);
 /* on != 0 (default): radix sequences and block widths L with a compile-time-
  * specialised kernel use it (FFT passes, Gram products, block updates) */
 int bdda_tune_fixed(int on);

@@ -67,3 +67,23 @@ def test_fp32_product_tracks_fp64(case):
     Y = _mvp(case, 0, case["S"])
     Y32 = _mvp(case, 1, case["S"])
     assert (Y32 - Y).abs().max().item() / Y.abs().max().item() < 2e-5
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_autotuned_launch_choices_keep_the_product(case, prec):
+    """The autotuner only changes launch shapes: every candidate it leaves in
+    place gives the same product, and it never ends slower than it started
+    by more than timing noise."""
+    from bdda_b200.runtime import autotune
+    lib = case["lib"].load()
+    Y0 = _mvp(case, prec, case["S"])
+    before, after = autotune(case["green"], case["occ"], 64, prec, reps=2)
+    assert after <= 1.05 * before
+    import ctypes as C
+    lt, var = C.c_int(), C.c_int()
+    mx = case["plan"].m[0]
+    assert lib.bdda_tune_pass_get(prec, 1, mx, 64, C.byref(lt), C.byref(var)) == 0
+    assert lt.value in (2, 4, 8) and var.value >= -1
+    Y1 = _mvp(case, prec, case["S"])
+    tol = 1e-12 if prec == 0 else 2e-5
+    assert (Y1 - Y0).abs().max().item() / Y0.abs().max().item() < tol
