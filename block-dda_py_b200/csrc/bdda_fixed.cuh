@@ -63,8 +63,8 @@ __global__ void __launch_bounds__(NT, MINB) fixed_pencil_kernel(const PassArgs a
   extern __shared__ __align__(16) unsigned char smraw[];
   T *tw, *sm, *gs;
   int32_t* cm;
-  stage_constants<T, KIND, LT>(a, smraw, RS::M, &tw, &sm, &gs, &cm);
-  const Pen c = pen_of_block<T>(a, cm);
+  stage_constants<T, KIND, LT>(a, smraw, RS::M, &tw, &sm, &gs, &cm, blockIdx.x);
+  const Pen c = pen_of_block<T>(a, cm, blockIdx.x);
   if constexpr (KIND == K_FWD) {
     if constexpr (N == 1) {
       fixed_stage<RS, 0, false, 1, 1, KIND, T, LT, NT>(a, c, sm, tw);

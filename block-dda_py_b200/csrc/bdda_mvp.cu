@@ -25,73 +25,11 @@
 
 namespace bdda {
 
-// Generic pencil kernel: runtime radix sequence (any length factored into
-// radices <= RadixCap).  The specialised kernels (bdda_fixed_*.cu) replace it
-// for the radix sequences the workloads use.
+// Generic pencil kernel, one item per CTA.
 template <typename T, int KIND, int LT>
 __global__ void __launch_bounds__(256) pencil_kernel(const PassArgs a) {
   extern __shared__ __align__(16) unsigned char smraw[];
-  const int M = a.ax.M, nst = a.ax.nst;
-  T *tw, *sm, *gs;
-  int32_t* cm;
-  stage_constants<T, KIND, LT>(a, smraw, M, &tw, &sm, &gs, &cm);
-  const Pen c = pen_of_block<T>(a, cm);
-  if constexpr (KIND == K_FWD) {
-    bool staged = false;
-    if constexpr (std::is_same<T, double2>::value) {
-      if (a.green) {   // real-space tensor rows evaluated into the tile (3 LT == 6)
-        for (int i = threadIdx.x; i < M; i += blockDim.x)
-          green_row(a, (int)c.p0, (int)c.p1, i, reinterpret_cast<double2*>(sm) + i * 3 * LT);
-        __syncthreads();
-        staged = true;
-      }
-    }
-    if (nst == 1) {
-      if (staged) run_stage<false, 0, 1, KIND, T, LT>(a, c, sm, tw, 0);
-      else run_stage<false, 1, 1, KIND, T, LT>(a, c, sm, tw, 0);
-      return;
-    }
-    if (staged) run_stage<false, 0, 0, KIND, T, LT>(a, c, sm, tw, 0);
-    else run_stage<false, 1, 0, KIND, T, LT>(a, c, sm, tw, 0);
-    __syncthreads();
-    for (int s = 1; s < nst - 1; ++s) {
-      run_stage<false, 0, 0, KIND, T, LT>(a, c, sm, tw, s);
-      __syncthreads();
-    }
-    run_stage<false, 0, 1, KIND, T, LT>(a, c, sm, tw, nst - 1);
-  } else if constexpr (KIND == K_INV) {
-    if (nst == 1) {
-      run_stage<true, 1, 1, KIND, T, LT>(a, c, sm, tw, 0);
-      return;
-    }
-    run_stage<true, 1, 0, KIND, T, LT>(a, c, sm, tw, nst - 1);
-    __syncthreads();
-    for (int s = nst - 2; s >= 1; --s) {
-      run_stage<true, 0, 0, KIND, T, LT>(a, c, sm, tw, s);
-      __syncthreads();
-    }
-    run_stage<true, 0, 1, KIND, T, LT>(a, c, sm, tw, 0);
-  } else {   // K_CONV
-    cp_async_wait<0>();
-    __syncthreads();
-    if (nst == 1) {
-      run_conv_mid<1, 1, T, LT>(a, c, sm, gs);
-      return;
-    }
-    run_stage<false, 1, 0, KIND, T, LT>(a, c, sm, tw, 0);
-    __syncthreads();
-    for (int s = 1; s < nst - 1; ++s) {
-      run_stage<false, 0, 0, KIND, T, LT>(a, c, sm, tw, s);
-      __syncthreads();
-    }
-    run_conv_mid<0, 0, T, LT>(a, c, sm, gs);
-    __syncthreads();
-    for (int s = nst - 2; s >= 1; --s) {
-      run_stage<true, 0, 0, KIND, T, LT>(a, c, sm, tw, s);
-      __syncthreads();
-    }
-    run_stage<true, 0, 1, KIND, T, LT>(a, c, sm, tw, 0);
-  }
+  generic_pencil<T, KIND, LT>(a, blockIdx.x, smraw);
 }
 
 template <typename T>

@@ -118,10 +118,10 @@ __host__ __device__ __forceinline__ int pencil_smem_bytes(int M, int LT, int kin
 
 // Pencil and tile of a CTA (one item per CTA).
 template <typename T>
-__device__ __forceinline__ Pen pen_of_block(const PassArgs& a, const int32_t* cm) {
+__device__ __forceinline__ Pen pen_of_block(const PassArgs& a, const int32_t* cm, int64_t bid) {
   Pen c;
-  c.tile = (int)(blockIdx.x % a.ntile);
-  const int64_t p = blockIdx.x / a.ntile;
+  c.tile = (int)(bid % a.ntile);
+  const int64_t p = bid / a.ntile;
   c.p0 = p / a.P1;
   c.p1 = p - c.p0 * a.P1;
   c.srcb = static_cast<const T*>(a.src) + c.p0 * a.src_p0 + c.p1 * a.src_p1;
@@ -134,7 +134,7 @@ __device__ __forceinline__ Pen pen_of_block(const PassArgs& a, const int32_t* cm
 // for the X pass, the Green's pencil).  Returns after the twiddles landed.
 template <typename T, int KIND, int LT>
 __device__ __forceinline__ void stage_constants(const PassArgs& a, unsigned char* smraw, int M, T** tw, T** sm,
-                                                T** gs, int32_t** cm) {
+                                                T** gs, int32_t** cm, int64_t bid) {
   const int o_sm = align16(M * (int)sizeof(T));
   const int o_gs = o_sm + align16(M * 3 * LT * (int)sizeof(T));
   const int o_cm = o_gs + (KIND == K_CONV ? align16(M * 6 * (int)sizeof(T)) : 0);
@@ -145,12 +145,12 @@ __device__ __forceinline__ void stage_constants(const PassArgs& a, unsigned char
   async_copy(*tw, a.tw, M * (int)sizeof(T));
   cp_async_commit();
   if constexpr (KIND == K_CONV) {
-    const int64_t p = blockIdx.x / a.ntile;
+    const int64_t p = bid / a.ntile;
     async_copy(*gs, static_cast<const T*>(a.ghat) + p * (int64_t)M * 6, M * 6 * (int)sizeof(T));
   }
   cp_async_commit();
   if (a.cell_map) {   // the pencil's occupancy-map rows (Z and Z^-1 passes)
-    const int64_t p = blockIdx.x / a.ntile;
+    const int64_t p = bid / a.ntile;
     const int64_t p0 = p / a.P1, p1 = p - p0 * a.P1;
     const int32_t* src = a.cell_map + p0 * a.cell_p0 + p1 * a.cell_p1;
     const int rows = KIND == K_INV ? a.n_out : a.n_in;
@@ -340,6 +340,75 @@ __device__ void run_conv_mid(const PassArgs& a, const Pen& c, T* sm, const T* gs
 #undef BDDA_MID_CASE
       default: break;
     }
+  }
+}
+
+// Generic pencil pass of CTA-sized item bid: runtime radix sequence (any
+// length factored into radices <= RadixCap).  The specialised kernels
+// (bdda_fixed_*.cu) replace it for the radix sequences the workloads use; the
+// batched solver runs it from persistent CTAs.
+template <typename T, int KIND, int LT>
+__device__ __forceinline__ void generic_pencil(const PassArgs& a, int64_t bid, unsigned char* smraw) {
+  const int M = a.ax.M, nst = a.ax.nst;
+  T *tw, *sm, *gs;
+  int32_t* cm;
+  stage_constants<T, KIND, LT>(a, smraw, M, &tw, &sm, &gs, &cm, bid);
+  const Pen c = pen_of_block<T>(a, cm, bid);
+  if constexpr (KIND == K_FWD) {
+    bool staged = false;
+    if constexpr (std::is_same<T, double2>::value) {
+      if (a.green) {   // real-space tensor rows evaluated into the tile (3 LT == 6)
+        for (int i = threadIdx.x; i < M; i += blockDim.x)
+          green_row(a, (int)c.p0, (int)c.p1, i, reinterpret_cast<double2*>(sm) + i * 3 * LT);
+        __syncthreads();
+        staged = true;
+      }
+    }
+    if (nst == 1) {
+      if (staged) run_stage<false, 0, 1, KIND, T, LT>(a, c, sm, tw, 0);
+      else run_stage<false, 1, 1, KIND, T, LT>(a, c, sm, tw, 0);
+      return;
+    }
+    if (staged) run_stage<false, 0, 0, KIND, T, LT>(a, c, sm, tw, 0);
+    else run_stage<false, 1, 0, KIND, T, LT>(a, c, sm, tw, 0);
+    __syncthreads();
+    for (int s = 1; s < nst - 1; ++s) {
+      run_stage<false, 0, 0, KIND, T, LT>(a, c, sm, tw, s);
+      __syncthreads();
+    }
+    run_stage<false, 0, 1, KIND, T, LT>(a, c, sm, tw, nst - 1);
+  } else if constexpr (KIND == K_INV) {
+    if (nst == 1) {
+      run_stage<true, 1, 1, KIND, T, LT>(a, c, sm, tw, 0);
+      return;
+    }
+    run_stage<true, 1, 0, KIND, T, LT>(a, c, sm, tw, nst - 1);
+    __syncthreads();
+    for (int s = nst - 2; s >= 1; --s) {
+      run_stage<true, 0, 0, KIND, T, LT>(a, c, sm, tw, s);
+      __syncthreads();
+    }
+    run_stage<true, 0, 1, KIND, T, LT>(a, c, sm, tw, 0);
+  } else {   // K_CONV
+    cp_async_wait<0>();
+    __syncthreads();
+    if (nst == 1) {
+      run_conv_mid<1, 1, T, LT>(a, c, sm, gs);
+      return;
+    }
+    run_stage<false, 1, 0, KIND, T, LT>(a, c, sm, tw, 0);
+    __syncthreads();
+    for (int s = 1; s < nst - 1; ++s) {
+      run_stage<false, 0, 0, KIND, T, LT>(a, c, sm, tw, s);
+      __syncthreads();
+    }
+    run_conv_mid<0, 0, T, LT>(a, c, sm, gs);
+    __syncthreads();
+    for (int s = nst - 2; s >= 1; --s) {
+      run_stage<true, 0, 0, KIND, T, LT>(a, c, sm, tw, s);
+      __syncthreads();
+    }
+    run_stage<true, 0, 1, KIND, T, LT>(a, c, sm, tw, 0);
   }
 }
 
