@@ -290,7 +290,7 @@ def run_bdda(args, rank, world, local_rank):
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(ms, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "complex64 Krylov + complex128 refinement" if mixed else "complex128",
+        "dtype": "complex64 products, complex128 Krylov + true residual" if mixed else "complex128",
         "form": args.form,
         "data": "synthetic: reference GRE geometry (seed 1) and SO(3) orientations (seed 2)",
         "config": dict(workload_config(L), parallelism="replicas x%d" % world,
@@ -413,6 +413,118 @@ def run_mvp_only(args):
                       "passes_GBs": [round(b / (t * 1e-3) / 1e9, 1) for b, t in zip(pb, per)]}), flush=True)
 
 
+# ---------------------------------------------------------------------------
+# batched uneven sweep: 48 GRE particles x 3 wavelengths, L = 32
+# ---------------------------------------------------------------------------
+SWEEP_WL = (0.45, 0.55, 0.85)
+SWEEP_MP = 1.53 + 0.005j
+
+
+def sweep_shapes(n_particles, seed=3):
+    """Shape parameters of the sweep: x ~ U[4,16], ab, bc ~ U[0.5,1], beta ~ U[0,0.2]."""
+    rng = np.random.default_rng(seed)
+    x = rng.uniform(4.0, 16.0, n_particles)
+    ab = rng.uniform(0.5, 1.0, n_particles)
+    bc = rng.uniform(0.5, 1.0, n_particles)
+    beta = rng.uniform(0.0, 0.2, n_particles)
+    return [dict(x=float(x[i]), ab=float(ab[i]), bc=float(bc[i]), beta=float(beta[i]), seed=1000 * seed + i)
+            for i in range(n_particles)]
+
+
+def _sweep_geometry(spec):
+    from bdda_b200.shapes import gre_particle
+    g = gre_particle(spec["x"], spec["ab"], spec["bc"], spec["beta"], spec["seed"], wl_0=1.0, m_m=1.0, workers=1)
+    return {k: g[k] for k in ("lattice_n", "lattice_lf", "is_in", "grid")}
+
+
+def run_sweep(args):
+    """Orientations/s of the sweep: one problem at a time vs one batched solve, FP64 and mixed."""
+    import concurrent.futures
+    import multiprocessing
+    specs = sweep_shapes(args.sweep_particles)
+    t0 = time.perf_counter()
+    # shapes on the host cores, before any CUDA call: spawned single-threaded workers
+    for var in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS"):
+        os.environ[var] = "1"
+    with concurrent.futures.ProcessPoolExecutor(max_workers=max(1, min(32, (os.cpu_count() or 2) - 1)),
+                                                mp_context=multiprocessing.get_context("spawn")) as ex:
+        geos = list(ex.map(_sweep_geometry, specs))
+    shape_s = time.perf_counter() - t0
+    import torch
+    from bdda_b200 import _lib
+    from bdda_b200.inputs import so3_euler
+    from bl_dda import scatterer as sc
+    sc.DiscreteDipoles.verbose = False
+    lib = _lib.load()
+    L = 32
+    problems = []
+    for i, g in enumerate(geos):
+        for j, wl in enumerate(SWEEP_WL):
+            lf = g["lattice_lf"] * wl      # the shape scales with the wavelength (spacing lambda/16)
+            t = sc.Target("gre%d" % i, g["lattice_n"], lf, g["grid"] * wl, g["is_in"], [SWEEP_MP] * 3)
+            problems.append((t, sc.IncidentField(wl, 1.0, so3_euler(L, 300 + 3 * i + j))))
+    n_dip = [int(g["is_in"].sum()) for g in geos]
+    t0 = time.perf_counter()
+    dds = []
+    for t, inc in problems:
+        d = sc.DiscreteDipoles(t, inc)
+        d.tol, d.itermax = TOL, ITERMAX
+        d.set_interaction_matrix()
+        dds.append(d)
+    greens = [d.Au_til for d in dds]
+    torch.cuda.synchronize()
+    green_s = time.perf_counter() - t0
+
+    def arm(batched, precision):
+        for d in dds:
+            d.precision = precision
+        torch.cuda.synchronize()
+        n0 = lib.bdda_launch_count()
+        t0 = time.perf_counter()
+        for d, g in zip(dds, greens):
+            d.set_interaction_matrix(green=g)
+        if batched:
+            sc.solve_matrix_equations(dds)
+        else:
+            for d in dds:
+                d.solve_matrix_equation()
+        obs = [d.observables() for d in dds]
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        return dict(value=round(len(dds) * L / dt, 2), seconds=round(dt, 3),
+                    launches=int(lib.bdda_launch_count() - n0),
+                    converged=int(sum(d.converge for d in dds)),
+                    iterations_mean=round(float(np.mean([d.iter_fin + 1 for d in dds])), 2)), obs
+
+    arm(True, "mixed")                      # warm-up (graphs, kernels, allocator)
+    res = {}
+    obs = {}
+    for name, batched, prec in (("one_at_a_time_fp64", False, None), ("one_at_a_time_mixed", False, "mixed"),
+                                ("batched_fp64", True, None), ("batched_mixed", True, "mixed")):
+        res[name], obs[name] = arm(batched, prec)
+    ref = obs["one_at_a_time_fp64"]
+    err = 0.0
+    for o, r in zip(obs["batched_mixed"], ref):
+        for cols in ((1,), (2, 3), (4, 5), (10, 11)):
+            a = o[:, cols[0]] + (1j * o[:, cols[1]] if len(cols) > 1 else 0)
+            b = r[:, cols[0]] + (1j * r[:, cols[1]] if len(cols) > 1 else 0)
+            err = max(err, float(np.max(np.abs(a - b)) / np.max(np.abs(b))))
+    out = {"metric": "orientations/s over a batched uneven sweep to rel-res 1e-5", "unit": "orientations/s",
+           "config": {"workload": "%d GRE particles (x~U[4,16], ab,bc~U[0.5,1], beta~U[0,0.2], seed 3) x "
+                                  "wavelengths %s, m_m 1, m_p %s, lambda/16 spacing, L=%d, block-BiCGSTAB"
+                                  % (len(geos), list(SWEEP_WL), SWEEP_MP, L),
+                      "problems": len(dds), "lattices_min_max": [min(int(np.prod(g["lattice_n"])) for g in geos),
+                                                                 max(int(np.prod(g["lattice_n"])) for g in geos)],
+                      "dipoles_min_max": [min(n_dip), max(n_dip)]},
+           "arms": res, "speedup_batched_mixed_vs_one_at_a_time_fp64":
+               round(res["batched_mixed"]["value"] / res["one_at_a_time_fp64"]["value"], 3),
+           "speedup_batched_vs_one_at_a_time_mixed":
+               round(res["batched_mixed"]["value"] / res["one_at_a_time_mixed"]["value"], 3),
+           "max_rel_err_batched_mixed_vs_fp64_observables": float("%.3g" % err),
+           "setup_s": {"shapes_host": round(shape_s, 2), "green_spectra": round(green_s, 2)}}
+    print(json.dumps(out), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -425,7 +537,13 @@ def main():
     ap.add_argument("--L", type=int, default=64)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--mvp-only", action="store_true", help="time block MVPs of the workload only")
+    ap.add_argument("--sweep", action="store_true",
+                    help="batched uneven sweep (48 GRE particles x 3 wavelengths, L=32) instead of the headline")
+    ap.add_argument("--sweep-particles", type=int, default=48)
     args = ap.parse_args()
+    if args.sweep:
+        run_sweep(args)
+        return
     if args.mvp_only:
         run_mvp_only(args)
         return

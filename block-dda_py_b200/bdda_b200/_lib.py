@@ -18,6 +18,8 @@ LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libbdda.so"
 OK, NOT_CONVERGED, BREAKDOWN, BAD_ARG, NO_WORKSPACE, TIMEOUT, CUDA_ERROR = range(7)
 # precisions (include/bdda.h: enum bdda_precision)
 C128, C64 = 0, 1
+# batched solve modes (include/bdda.h: enum bdda_batch_mode)
+BATCH_C128, BATCH_C64, BATCH_MIXED = 0, 1, 2
 # solvers (include/bdda.h: enum bdda_solver_kind)
 BICGSTAB, COCG_RQ = 0, 1
 
@@ -37,6 +39,11 @@ PROTOTYPES = {
     "bdda_tune_get": (_i, [_i, _i, C.POINTER(_sz), _pi]),
     "bdda_tune_fixed": (_i, [_i]),
     "bdda_tune_pass": (_i, [_i, _i, _i, _i, _i, _i]),
+    "bdda_batch_workspace_bytes": (_sz, [_vp, _i, _i, _i, _i]),
+    "bdda_mixed_workspace_bytes": (_sz, [_vp, _i, _i]),
+    "bdda_mixed_solve": (_i, [_vp, _i, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _d, _i, _i, _vp, _pi, _pd, _pd,
+                              _vp, _sz, _vp]),
+    "bdda_batch_bicgstab": (_i, [_vp, _i, _i, _i, _d, _i, _i, _i, _pi, _pi, _pd, _pd, _vp, _sz, _vp]),
     "bdda_tune_pass_get": (_i, [_i, _i, _i, _i, _pi, _pi]),
     "bdda_autotune": (_i, [_vp, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i, _pd, _pd, _vp]),
     "bdda_plan_create": (_i, [_pi, _pi, C.POINTER(_vp)]),

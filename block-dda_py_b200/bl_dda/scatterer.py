@@ -287,3 +287,48 @@ class DiscreteDipoles(Target, IncidentField):
         self.S_bk_OCBS_phi = o[:, 8] + 1j * o[:, 9]
         self.S_bk_OCBS = o[:, 10] + 1j * o[:, 11]
         return self.S_bk_OCBS
+
+
+def solve_matrix_equations(dds, X0s=None, precision=None, graph=True):
+    """``solve_matrix_equation`` for many ``DiscreteDipoles`` in one batched call.
+
+    No counterpart in the reference, which solves one particle, wavelength
+    and orientation block at a time (run_dda.py:56-65).  Every object must
+    have had ``set_interaction_matrix()``; they may differ in lattice,
+    wavelength and refractive index but share L (8, 16, 32 or 64), ``tol``
+    and ``itermax``.  Block-BiCGSTAB (the reference's solver) through
+    ``bl_krylov.bl_bicgstab_jacobi_mvp_fft_batch``; ``precision`` as there
+    (default: each object's ``precision``, which must agree).  Sets
+    ``X``/``P``/``E``, ``iter_fin``, ``err_fin`` and ``converge`` of each.
+    """
+    dds = list(dds)
+    if not dds:
+        return
+    tols = {float(d.tol) for d in dds}
+    itms = {int(d.itermax) for d in dds}
+    if len(tols) != 1 or len(itms) != 1:
+        raise ValueError("batched objects must share tol and itermax")
+    if precision is None:
+        precs = {d.precision for d in dds}
+        if len(precs) != 1:
+            raise ValueError("batched objects must share precision")
+        precision = precs.pop()
+    probs = []
+    for i, d in enumerate(dds):
+        if d.Au_til is None:
+            raise ValueError("call set_interaction_matrix() first")
+        p = (d.lattice_n, d._dev["occ"], d.Au_til, d._dev["diag"], d._dev["B"])
+        x0 = None if X0s is None else X0s[i]
+        probs.append(p if x0 is None else p + (x0,))
+    start = time.time()
+    res = bl_krylov.bl_bicgstab_jacobi_mvp_fft_batch(probs, tols.pop(), itms.pop(), precision=precision,
+                                                     graph=graph)
+    for d, (X, it, err) in zip(dds, res):
+        d.iter_fin, d.err_fin = it, err
+        d._dev["X"] = X
+        d._host.pop("X", None)
+        d._obs = None
+        d.converge = bool(err < d.tol)
+    if DiscreteDipoles.verbose:
+        print("batched block-BiCGStab: %d problems, %d converged, solver time=%.1fs"
+              % (len(dds), sum(d.converge for d in dds), time.time() - start))

@@ -58,7 +58,11 @@ def _block_mvp(n, f, Au_til, full_idx, DIAG_A, S, jpre, precision=None):
     return out.cpu().numpy() if to_numpy else out
 
 
-MIXED = ("mixed", "c64-refine", "fp32-refine", "mixed-reliable")
+# "mixed": complex128 Krylov vectors, complex64 products, complex128 true residual
+# (bdda_mixed_solve); "mixed-fp32": complex64 vectors and products restarted
+# inside FP64 refinement (bdda_refine_solve); "mixed-reliable": one complex64
+# recursion with FP64 residual replacement (BiCGSTAB)
+MIXED = ("mixed", "mixed-fp32", "c64-refine", "fp32-refine", "mixed-reliable")
 
 
 def _solve(kind, n, f, address, Au_til, DIAG_A, B, tol, itermax, X0=None, precision=None,
@@ -89,7 +93,15 @@ def _solve(kind, n, f, address, Au_til, DIAG_A, B, tol, itermax, X0=None, precis
     hist = (C.c_double * max(itermax, 1))()
     it = C.c_int(0)
     err = C.c_double(float("inf"))
-    if mixed:
+    if mixed and precision.lower() == "mixed":
+        nbytes = int(lib.bdda_mixed_workspace_bytes(plan.handle, L, occ.n_occ))
+        work = torch.empty(max(nbytes, 16), dtype=torch.uint8, device=plan.device)
+        status = lib.bdda_mixed_solve(plan.handle, kind, L, occ.n_occ, ptr(g.ghat(_lib.C128)),
+                                      ptr(g.ghat(_lib.C64)), ptr(occ.cell_map), ptr(diag), ptr(Bd), ptr(X0d),
+                                      float(tol), itermax, abs(int(max_outer)), ptr(X), C.byref(it),
+                                      C.byref(err), hist, ptr(work), nbytes, stream_ptr(plan.device))
+        _lib.check(status, "bdda_mixed_solve")
+    elif mixed:
         nbytes = int(lib.bdda_refine_workspace_bytes(plan.handle, L, occ.n_occ))
         work = torch.empty(max(nbytes, 16), dtype=torch.uint8, device=plan.device)
         status = lib.bdda_refine_solve(plan.handle, kind, L, occ.n_occ, ptr(g.ghat(_lib.C128)),
@@ -125,11 +137,14 @@ def bl_cocg_rq_jacobi_mvp_fft(n, f, address, Au_til, DIAG_A, B, tol, itermax, X0
     (f*N_occ, L) solution, iter_fin the 0-based index of the last iteration,
     err_fin = ||xi||_F / ||M^-1 B||_F at that iteration.  Not converging is
     not an error.  Extra keywords (all optional): ``X0`` initial guess,
-    ``precision`` "c128" (default), "c64" (FP32 throughout), "mixed" (FP32
-    block solves restarted inside an FP64 iterative refinement; err_fin is
-    then the true residual ||M^-1 (B - A X)|| / ||M^-1 B||; ``inner_tol``
-    and ``max_outer`` tune it) or, for BiCGSTAB, "mixed-reliable" (one FP32
-    recursion with FP64 residual replacement, for small L), ``history``
+    ``precision`` "c128" (default), "c64" (FP32 throughout), "mixed"
+    (complex128 Krylov vectors and small solves, complex64 products, the
+    complex128 true residual judged at the end with warm restarts; err_fin
+    is then the true residual ||M^-1 (B - A X)|| / ||M^-1 B||), "mixed-fp32"
+    (complex64 block solves restarted inside an FP64 iterative refinement;
+    ``inner_tol`` and ``max_outer`` tune it) or, for BiCGSTAB,
+    "mixed-reliable" (one FP32 recursion with FP64 residual replacement, for
+    small L), ``history``
     list receiving the per-iteration residuals, ``verbose`` prints them like
     the reference.
     The QR factorisations are CholeskyQR (R with real positive diagonal
@@ -151,3 +166,156 @@ def bl_bicgstab_jacobi_mvp_fft(n, f, address, Au_til, DIAG_A, B, tol, itermax, X
     """
     return _solve(_lib.BICGSTAB, n, f, address, Au_til, DIAG_A, B, tol, itermax, X0, precision,
                   history, verbose, inner_tol, max_outer)
+
+
+# ---- batched solves (no reference counterpart: the reference solves one problem per call) ----
+class _BatchProblem(C.Structure):
+    """include/bdda.h: bdda_batch_problem."""
+    _fields_ = [("plan", C.c_void_p), ("n_occ", C.c_int), ("ghat", C.c_void_p), ("ghat_c64", C.c_void_p),
+                ("cell_map", C.c_void_p), ("diag", C.c_void_p), ("B", C.c_void_p), ("X0", C.c_void_p),
+                ("X", C.c_void_p)]
+
+
+_BATCH_MODES = {"c128": _lib.BATCH_C128, "fp64": _lib.BATCH_C128, "complex128": _lib.BATCH_C128,
+                "c64": _lib.BATCH_C64, "fp32": _lib.BATCH_C64, "complex64": _lib.BATCH_C64,
+                "mixed": _lib.BATCH_MIXED}
+
+
+def _batch_entry(p):
+    if isinstance(p, dict):
+        n, address, Au_til, DIAG_A, B, X0 = (p["n"], p["address"], p["Au_til"], p["DIAG_A"], p["B"],
+                                              p.get("X0"))
+    else:
+        n, address, Au_til, DIAG_A, B = p[:5]
+        X0 = p[5] if len(p) > 5 else None
+    g = as_green(n, Au_til)
+    plan = g.plan
+    occ = address if isinstance(address, Occupancy) else Occupancy(plan, address)
+    to_numpy = not isinstance(B, torch.Tensor)
+    Bd = to_device(B, torch.complex128, plan.device)
+    if Bd.dim() != 2 or Bd.shape[0] != 3 * occ.n_occ:
+        raise ValueError("B must be (%d, L), got %r" % (3 * occ.n_occ, tuple(Bd.shape)))
+    diag = to_device(DIAG_A, torch.complex128, plan.device).reshape(-1)
+    if diag.numel() != 3 * occ.n_occ:
+        raise ValueError("DIAG_A must have %d entries" % (3 * occ.n_occ))
+    X0d = None if X0 is None else to_device(X0, torch.complex128, plan.device).reshape(Bd.shape).contiguous()
+    return dict(g=g, occ=occ, B=Bd, diag=diag, X0=X0d, X=torch.empty_like(Bd), numpy=to_numpy)
+
+
+def _batch_struct(entries, mode):
+    arr = (_BatchProblem * len(entries))()
+    for i, e in enumerate(entries):
+        g = e["g"]
+        s = arr[i]
+        s.plan = g.plan.handle.value
+        s.n_occ = e["occ"].n_occ
+        s.ghat = ptr(g.ghat(_lib.C128)) if mode != _lib.BATCH_C64 else None
+        s.ghat_c64 = ptr(g.ghat(_lib.C64)) if mode != _lib.BATCH_C128 else None
+        s.cell_map = ptr(e["occ"].cell_map)
+        s.diag = ptr(e["diag"])
+        s.B = ptr(e["B"])
+        s.X0 = ptr(e["X0"])
+        s.X = ptr(e["X"])
+    return arr
+
+
+def _batch_groups(entries, mode, L, itermax, max_bytes):
+    """Consecutive groups whose workspace fits max_bytes (at most 1024 problems each)."""
+    lib = _lib.load()
+    groups, cur = [], []
+    for e in entries:
+        trial = cur + [e]
+        nbytes = int(lib.bdda_batch_workspace_bytes(_batch_struct(trial, mode), len(trial), mode, L, itermax))
+        if cur and (len(trial) > 1024 or nbytes > max_bytes):
+            groups.append(cur)
+            cur = [e]
+        else:
+            cur = trial
+    if cur:
+        groups.append(cur)
+    return groups
+
+
+def bl_bicgstab_jacobi_mvp_fft_batch(problems, tol, itermax, precision=None, max_outer=20,
+                                     graph=True, history=None, statuses=None, max_bytes=None):
+    """Block-BiCGSTAB (bl_krylov.py:121-187) on many independent problems at once.
+
+    ``problems``: a sequence of ``(n, address, Au_til, DIAG_A, B)`` or
+    ``(n, address, Au_til, DIAG_A, B, X0)`` tuples (or dicts with those keys),
+    each exactly the arguments of :func:`bl_bicgstab_jacobi_mvp_fft` for one
+    particle / wavelength / orientation block; grids may differ, L (the
+    columns of B) is shared and is 8, 16, 32 or 64.  Returns one
+    ``(X, iter_fin, err_fin)`` per problem, with the meaning of the one-problem
+    solver.  ``precision``: "c128" (default), "c64", or "mixed" (complex128
+    Krylov vectors with complex64 products, judged on the complex128 true
+    residual, at most ``max_outer`` warm-restarted rounds; problems it leaves
+    above ``tol`` are solved again in complex128, iter_fin counting both).
+    ``graph``
+    replays the batched iteration as a CUDA graph.  ``history`` (list)
+    receives one residual list per problem, ``statuses`` (list) one status
+    code per problem.  A problem whose small system is singular raises
+    numpy.linalg.LinAlgError after the batch finished, unless ``statuses`` is
+    given, in which case its X is None.  Problems are split into groups whose
+    device workspace stays under ``max_bytes`` (default: 70 % of the free
+    device memory).
+    """
+    key = "c128" if precision is None else str(precision).lower()
+    if key not in _BATCH_MODES:
+        raise ValueError("precision must be one of %s" % sorted(_BATCH_MODES))
+    mode = _BATCH_MODES[key]
+    entries = [_batch_entry(p) for p in problems]
+    if not entries:
+        return []
+    Ls = {int(e["B"].shape[1]) for e in entries}
+    if len(Ls) != 1 or next(iter(Ls)) not in (8, 16, 32, 64):
+        raise ValueError("all problems need the same L, one of 8, 16, 32, 64 (got %s)" % sorted(Ls))
+    L = Ls.pop()
+    itermax = int(itermax)
+    dev = entries[0]["g"].plan.device
+    if max_bytes is None:
+        free, _ = torch.cuda.mem_get_info(dev)
+        max_bytes = int(0.7 * free)
+    lib = _lib.load()
+    results = []
+    for grp in _batch_groups(entries, mode, L, itermax, max_bytes):
+        arr = _batch_struct(grp, mode)
+        nb = int(lib.bdda_batch_workspace_bytes(arr, len(grp), mode, L, itermax))
+        if nb == 0:
+            raise ValueError("bdda_batch_workspace_bytes rejected the batch")
+        work = torch.empty(nb, dtype=torch.uint8, device=dev)
+        st = (C.c_int * len(grp))()
+        it = (C.c_int * len(grp))()
+        er = (C.c_double * len(grp))()
+        hist = (C.c_double * (len(grp) * max(itermax, 1)))() if history is not None else None
+        rc = lib.bdda_batch_bicgstab(arr, len(grp), mode, L, float(tol), itermax, int(max_outer),
+                                     1 if graph else 0, st, it, er, hist, ptr(work), nb, stream_ptr(dev))
+        if rc not in (0, 1, 2):
+            _lib.check(rc, "bdda_batch_bicgstab")
+        del work
+        for i, e in enumerate(grp):
+            s = int(st[i])
+            X = None if s == 2 else (e["X"].cpu().numpy() if e["numpy"] else e["X"])
+            results.append((X, int(it[i]), float(er[i]), s))
+            if history is not None:
+                ran = 0 if itermax == 0 or s == 2 else int(it[i]) + 1
+                history.append([hist[i * itermax + k] for k in range(min(ran, itermax))])
+    if mode == _lib.BATCH_MIXED:
+        # problems the mixed form leaves above tol (its recursion diverged under the
+        # complex64 products) are solved again with complex128 products
+        redo = [i for i, r in enumerate(results) if r[3] == 1 and not r[2] < tol]
+        if redo:
+            sub_hist = [] if history is not None else None
+            sub_st = []
+            again = bl_bicgstab_jacobi_mvp_fft_batch([problems[i] for i in redo], tol, itermax, "c128",
+                                                     max_outer, graph, sub_hist, sub_st, max_bytes)
+            for j, i in enumerate(redo):
+                X, it, er = again[j]
+                results[i] = (X, results[i][1] + 1 + it, er, sub_st[j])
+                if history is not None:
+                    history[i] = history[i] + sub_hist[j]
+    if statuses is not None:
+        statuses.extend(r[3] for r in results)
+    elif any(r[3] == 2 for r in results):
+        bad = [i for i, r in enumerate(results) if r[3] == 2]
+        raise np.linalg.LinAlgError("Singular matrix in batched problems %s" % bad)
+    return [r[:3] for r in results]

@@ -163,12 +163,11 @@ template <> struct TwOff<float2> { static size_t get(const bdda_plan* p, int ax)
     if (s_ != BDDA_OK) return s_;    \
   } while (0)
 
-// The five passes.  cell_map == nullptr: dense cuboid in and out, no epilogue
-// (fft_mvp); otherwise the sparse block MVP with diagonal and Jacobi scaling.
+// Arguments of the five passes of one product (without launch shape) and
+// the pencil-index extent P0 of each: Z, Y, X, Y^-1, Z^-1.
 template <typename T>
-static int run_mvp(const bdda_plan* plan, int L, const T* ghat, const int32_t* cell_map,
-                   const T* src, const T* diag, const T* jpre, T* out, T* F, cudaStream_t st,
-                   cudaEvent_t* ev = nullptr) {
+void mvp_pass_args(const bdda_plan* plan, int L, const T* ghat, const int32_t* cell_map, const T* src,
+                   const T* diag, const T* jpre, T* out, T* F, PassArgs a[5], int64_t P0[5]) {
   const int64_t Nx = plan->n[0], Ny = plan->n[1], Nz = plan->n[2];
   const int64_t Mx = plan->ax[0].M, My = plan->ax[1].M, Mz = plan->ax[2].M;
   const int64_t C = 3 * (int64_t)L;
@@ -177,63 +176,75 @@ static int run_mvp(const bdda_plan* plan, int L, const T* ghat, const int32_t* c
   b.L = L;
   b.C = C;
   b.scale = 1.0;
-  const bool prof = profiling();
-  if (prof) profile_mark(0, st, prec_of<T>());
-  if (ev) BDDA_CUDA_TRY(cudaEventRecord(ev[0], st));
-
   {  // Z: gather + forward z
-    PassArgs a = b;
-    a.ax = plan->ax[2]; a.tw = table_ptr<T>(plan, TwOff<T>::get(plan, 2));
-    a.n_in = (int)Nz; a.n_out = (int)Mz; a.P1 = (int)Ny;
-    a.cell_map = cell_map; a.cell_p0 = Ny * Nz; a.cell_p1 = Nz;
-    a.S = src;
-    a.src = src; a.src_p0 = Ny * Nz * C; a.src_p1 = Nz * C; a.src_row = C;   // dense cuboid input
-    a.dst = F; a.dst_p0 = My * Mz * C; a.dst_p1 = Mz * C; a.dst_row = C;
-    BDDA_TRY((launch_pass<T, K_FWD>(a, Nx, pick_lt<T>((int)Mz, L, K_FWD), st)));
-    if (prof) profile_mark(1, st);
-    if (ev) BDDA_CUDA_TRY(cudaEventRecord(ev[1], st));
+    PassArgs& q = a[0];
+    q = b;
+    q.ax = plan->ax[2]; q.tw = table_ptr<T>(plan, TwOff<T>::get(plan, 2));
+    q.n_in = (int)Nz; q.n_out = (int)Mz; q.P1 = (int)Ny;
+    q.cell_map = cell_map; q.cell_p0 = Ny * Nz; q.cell_p1 = Nz;
+    q.S = src;
+    q.src = src; q.src_p0 = Ny * Nz * C; q.src_p1 = Nz * C; q.src_row = C;   // dense cuboid input
+    q.dst = F; q.dst_p0 = My * Mz * C; q.dst_p1 = Mz * C; q.dst_row = C;
+    P0[0] = Nx;
   }
   PassArgs ay = b;  // Y and Y^-1 share the pencil geometry
   ay.ax = plan->ax[1]; ay.tw = table_ptr<T>(plan, TwOff<T>::get(plan, 1));
   ay.P1 = (int)Mz; ay.src = F; ay.dst = F;
   ay.src_p0 = ay.dst_p0 = My * Mz * C; ay.src_p1 = ay.dst_p1 = C; ay.src_row = ay.dst_row = Mz * C;
-  {
-    PassArgs a = ay;
-    a.n_in = (int)Ny; a.n_out = (int)My;
-    BDDA_TRY((launch_pass<T, K_FWD>(a, Nx, pick_lt<T>((int)My, L, K_FWD), st)));
-    if (prof) profile_mark(2, st);
-    if (ev) BDDA_CUDA_TRY(cudaEventRecord(ev[2], st));
-  }
+  a[1] = ay;
+  a[1].n_in = (int)Ny; a[1].n_out = (int)My;
+  P0[1] = Nx;
   {  // X: forward, Green multiply, inverse
-    PassArgs a = b;
-    a.ax = plan->ax[0]; a.tw = table_ptr<T>(plan, TwOff<T>::get(plan, 0));
-    a.n_in = (int)Nx; a.n_out = (int)Nx; a.P1 = (int)Mz;
-    a.src = F; a.dst = F;
-    a.src_p0 = a.dst_p0 = Mz * C; a.src_p1 = a.dst_p1 = C; a.src_row = a.dst_row = My * Mz * C;
-    a.ghat = ghat;
-    BDDA_TRY((launch_pass<T, K_CONV>(a, My, pick_lt<T>((int)Mx, L, K_CONV), st)));
-    if (prof) profile_mark(3, st);
-    if (ev) BDDA_CUDA_TRY(cudaEventRecord(ev[3], st));
+    PassArgs& q = a[2];
+    q = b;
+    q.ax = plan->ax[0]; q.tw = table_ptr<T>(plan, TwOff<T>::get(plan, 0));
+    q.n_in = (int)Nx; q.n_out = (int)Nx; q.P1 = (int)Mz;
+    q.src = F; q.dst = F;
+    q.src_p0 = q.dst_p0 = Mz * C; q.src_p1 = q.dst_p1 = C; q.src_row = q.dst_row = My * Mz * C;
+    q.ghat = ghat;
+    P0[2] = My;
   }
-  {
-    PassArgs a = ay;
-    a.n_in = (int)My; a.n_out = (int)Ny;
-    BDDA_TRY((launch_pass<T, K_INV>(a, Nx, pick_lt<T>((int)My, L, K_INV), st)));
-    if (prof) profile_mark(4, st);
-    if (ev) BDDA_CUDA_TRY(cudaEventRecord(ev[4], st));
-  }
+  a[3] = ay;
+  a[3].n_in = (int)My; a[3].n_out = (int)Ny;
+  P0[3] = Nx;
   {  // Z^-1 + crop + epilogue
-    PassArgs a = b;
-    a.ax = plan->ax[2]; a.tw = table_ptr<T>(plan, TwOff<T>::get(plan, 2));
-    a.n_in = (int)Mz; a.n_out = (int)Nz; a.P1 = (int)Ny;
-    a.src = F; a.src_p0 = My * Mz * C; a.src_p1 = Mz * C; a.src_row = C;
-    a.cell_map = cell_map; a.cell_p0 = Ny * Nz; a.cell_p1 = Nz;
-    a.S = src; a.diag = diag; a.jpre = jpre;
-    a.dst = out; a.dst_p0 = Ny * Nz * C; a.dst_p1 = Nz * C; a.dst_row = C;   // dense cuboid output
-    a.scale = 1.0 / (double)(Mx * My * Mz);
-    BDDA_TRY((launch_pass<T, K_INV>(a, Nx, pick_lt<T>((int)Mz, L, K_INV), st)));
-    if (prof) profile_mark(5, st);
-    if (ev) BDDA_CUDA_TRY(cudaEventRecord(ev[5], st));
+    PassArgs& q = a[4];
+    q = b;
+    q.ax = plan->ax[2]; q.tw = table_ptr<T>(plan, TwOff<T>::get(plan, 2));
+    q.n_in = (int)Mz; q.n_out = (int)Nz; q.P1 = (int)Ny;
+    q.src = F; q.src_p0 = My * Mz * C; q.src_p1 = Mz * C; q.src_row = C;
+    q.cell_map = cell_map; q.cell_p0 = Ny * Nz; q.cell_p1 = Nz;
+    q.S = src; q.diag = diag; q.jpre = jpre;
+    q.dst = out; q.dst_p0 = Ny * Nz * C; q.dst_p1 = Nz * C; q.dst_row = C;   // dense cuboid output
+    q.scale = 1.0 / (double)(Mx * My * Mz);
+    P0[4] = Nx;
+  }
+}
+template void mvp_pass_args<double2>(const bdda_plan*, int, const double2*, const int32_t*, const double2*,
+                                     const double2*, const double2*, double2*, double2*, PassArgs*, int64_t*);
+template void mvp_pass_args<float2>(const bdda_plan*, int, const float2*, const int32_t*, const float2*,
+                                    const float2*, const float2*, float2*, float2*, PassArgs*, int64_t*);
+
+// The five passes.  cell_map == nullptr: dense cuboid in and out, no epilogue
+// (fft_mvp); otherwise the sparse block MVP with diagonal and Jacobi scaling.
+template <typename T>
+static int run_mvp(const bdda_plan* plan, int L, const T* ghat, const int32_t* cell_map,
+                   const T* src, const T* diag, const T* jpre, T* out, T* F, cudaStream_t st,
+                   cudaEvent_t* ev = nullptr) {
+  PassArgs a[5];
+  int64_t P0[5];
+  mvp_pass_args<T>(plan, L, ghat, cell_map, src, diag, jpre, out, F, a, P0);
+  const bool prof = profiling();
+  if (prof) profile_mark(0, st, prec_of<T>());
+  if (ev) BDDA_CUDA_TRY(cudaEventRecord(ev[0], st));
+  for (int q = 0; q < 5; ++q) {
+    const int kind = kPassKind[q];
+    const int lt = pick_lt<T>(a[q].ax.M, L, kind);
+    if (kind == K_FWD) BDDA_TRY((launch_pass<T, K_FWD>(a[q], P0[q], lt, st)));
+    else if (kind == K_CONV) BDDA_TRY((launch_pass<T, K_CONV>(a[q], P0[q], lt, st)));
+    else BDDA_TRY((launch_pass<T, K_INV>(a[q], P0[q], lt, st)));
+    if (prof) profile_mark(q + 1, st);
+    if (ev) BDDA_CUDA_TRY(cudaEventRecord(ev[q + 1], st));
   }
   return BDDA_OK;
 }

@@ -412,6 +412,14 @@ __device__ __forceinline__ void generic_pencil(const PassArgs& a, int64_t bid, u
   }
 }
 
+// Pass kind of the five passes of a product: Z, Y, X, Y^-1, Z^-1.
+constexpr int kPassKind[5] = {K_FWD, K_FWD, K_CONV, K_INV, K_INV};
+
+// Arguments of the five passes of one block product (bdda_mvp.cu).
+template <typename T>
+void mvp_pass_args(const bdda_plan* plan, int L, const T* ghat, const int32_t* cell_map, const T* src,
+                   const T* diag, const T* jpre, T* out, T* F, PassArgs a[5], int64_t P0[5]);
+
 // Launch hook of a compile-time-specialised pencil kernel.
 typedef int (*FixedLaunchFn)(const PassArgs& a, int64_t P0, cudaStream_t st);
 struct FixedKernel {

@@ -224,11 +224,39 @@ struct Ctx {
   SolverState* st;
   cudaStream_t stream;
   size_t sm2, sm3;   // dynamic smem of the small kernels (2 or 3 L x L matrices)
+  // complex128 vectors with complex64 products (the mixed form): the product
+  // inside the iteration runs on these buffers; null = complex128 products
+  const float2* ghat32 = nullptr;
+  float2 *diag32 = nullptr, *jpre32 = nullptr, *in32 = nullptr, *out32 = nullptr;
+  bool diverged = false;   // set when the complex64-product recursion blew up
 };
 
+// The product in the vectors' own precision.
+template <typename T>
+static int mvp_exact(Ctx<T>& c, const T* in, T* out) {
+  return block_mvp_impl<T>(c.plan, c.L, c.ghat, c.cell_map, c.diag, c.jpre, in, out, c.field, c.stream);
+}
+
+// The product inside the iteration: complex64 arithmetic when the context
+// carries complex64 buffers (input rounded to complex64, output widened).
 template <typename T>
 static int mvp(Ctx<T>& c, const T* in, T* out) {
-  return block_mvp_impl<T>(c.plan, c.L, c.ghat, c.cell_map, c.diag, c.jpre, in, out, c.field, c.stream);
+  if constexpr (std::is_same<T, double2>::value) {
+    if (c.ghat32) {
+      const int64_t ne = c.n * c.L;
+      convert_in_kernel<float2><<<kRedBlocks, 256, 0, c.stream>>>(in, c.in32, ne);
+      count_launch();
+      BDDA_CUDA_TRY(cudaGetLastError());
+      const int s = block_mvp_impl<float2>(c.plan, c.L, c.ghat32, c.cell_map, c.diag32, c.jpre32, c.in32, c.out32,
+                                           reinterpret_cast<float2*>(c.field), c.stream);
+      if (s != BDDA_OK) return s;
+      convert_out_kernel<float2><<<kRedBlocks, 256, 0, c.stream>>>(c.out32, out, ne);
+      count_launch();
+      BDDA_CUDA_TRY(cudaGetLastError());
+      return BDDA_OK;
+    }
+  }
+  return mvp_exact(c, in, out);
 }
 
 template <typename T>
@@ -265,6 +293,15 @@ static int read_state(Ctx<T>& c, double* err, int* bad) {
     if (s_ != BDDA_OK) return s_; \
   } while (0)
 
+// Residual replacement in the mixed form: when the recursive residual has
+// dropped by this factor below its largest value since the last replacement
+// (or below tol), it is recomputed from X with the complex128 product.
+constexpr double kReplaceDrop = 1e-2;
+// ... and it is abandoned as diverged once the residual exceeds its smallest
+// value so far by this factor (block-BiCGSTAB on strongly scattering
+// particles can amplify the complex64 rounding of the products without bound).
+constexpr double kDivergeFactor = 1e3;
+
 // Block-BiCGSTAB (bl_krylov.py:121-187).  vec: 0 X, 1 R, 2 P, 3 R0, 4 V, 5 T, 6 Z, 7 Bj
 template <typename T>
 static int bicgstab_core(Ctx<T>& c, bool has_x0, double tol, int itermax, int* iter_fin,
@@ -278,8 +315,8 @@ static int bicgstab_core(Ctx<T>& c, bool has_x0, double tol, int itermax, int* i
   norm_kernel<<<1, 256, 0, c.stream>>>(reinterpret_cast<double*>(c.partial), kRedBlocks, c.st, 1);
   count_launch();
   BDDA_CUDA_TRY(cudaGetLastError());
-  if (has_x0) {   // R = M^-1 (B - A X0)
-    TRY(mvp<T>(c, X, V));
+  if (has_x0) {   // R = M^-1 (B - A X0), with the exact product
+    TRY(mvp_exact<T>(c, X, V));
     TRY(upd<T>(c, R, Bj, nullptr, V, c.sp.r, nullptr, nullptr, nullptr, nullptr, false));
   }
   TRY(upd<T>(c, P, R, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, false));
@@ -287,6 +324,8 @@ static int bicgstab_core(Ctx<T>& c, bool has_x0, double tol, int itermax, int* i
   *iter_fin = 0;
   *err_fin = INFINITY;
   double err = INFINITY;
+  double rmax = 0.0;        // largest residual since the last replacement
+  double rmin = INFINITY;   // smallest residual so far
   for (int k = 0; k < itermax; ++k) {
     TRY(mvp<T>(c, P, V));                                   // V = M^-1 A P
     TRY(gram2<T>(c, true, R0, V, R, c.sp.g2));              // R0^H V, R0^H R
@@ -310,11 +349,29 @@ static int bicgstab_core(Ctx<T>& c, bool has_x0, double tol, int itermax, int* i
     int bad = 0;
     TRY(read_state(c, &err, &bad));
     if (bad == 1) return BDDA_BREAKDOWN;
+    if (bad != 2 && c.ghat32 && (err < tol || err < kReplaceDrop * rmax)) {
+      // complex64 products: replace the recursive residual by the true one
+      // (complex128 product; Z is free until the next iteration), so the
+      // drift of the recursion stays at the level of the current residual
+      TRY(mvp_exact<T>(c, X, Z));
+      TRY(upd<T>(c, R, Bj, nullptr, Z, c.sp.r, nullptr, nullptr, nullptr, nullptr, true));
+      norm_kernel<<<1, 256, 0, c.stream>>>(reinterpret_cast<double*>(c.partial), kRedBlocks, c.st, 0);
+      count_launch();
+      BDDA_CUDA_TRY(cudaGetLastError());
+      TRY(read_state(c, &err, &bad));
+      rmax = err;
+    }
+    rmax = err > rmax ? err : rmax;
+    rmin = err < rmin ? err : rmin;
     if (hist) hist[k] = err;
     *iter_fin = k;
     *err_fin = err;
     if (bad == 2) return BDDA_NOT_CONVERGED;   // NaN/Inf reached: stop, reported as not converged
     if (err < tol) return BDDA_OK;
+    if (c.ghat32 && err > kDivergeFactor * rmin) {
+      c.diverged = true;
+      return BDDA_NOT_CONVERGED;
+    }
     // P = R + (P - zeta V) beta
     TRY(upd<T>(c, P, R, nullptr, nullptr, nullptr, P, V, &c.st->negzeta, c.sp.beta, false));
   }
@@ -356,7 +413,7 @@ static int cocg_core(Ctx<T>& c, bool has_x0, double tol, int itermax, int* iter_
   count_launch();
   BDDA_CUDA_TRY(cudaGetLastError());
   if (has_x0) {
-    TRY(mvp<T>(c, X, AS));
+    TRY(mvp_exact<T>(c, X, AS));
     TRY(upd<T>(c, W, Bj, nullptr, AS, c.sp.r, nullptr, nullptr, nullptr, nullptr, false));
   }
   // Q, xi = qr(W)   (bl_krylov.py:92)
@@ -743,6 +800,124 @@ static int run_refine(int solver, bool restart, const bdda_plan* p, int L, int n
   return status;
 }
 
+// ---- complex128 Krylov with complex64 products ------------------------------------
+// The block solver keeps X, the residual and every Krylov vector, Gram
+// product and L x L step in complex128 and computes the products inside the
+// iteration in complex64 (the product dominates the cost).  BiCGSTAB replaces
+// its recursive residual by the true one (complex128 product) whenever it
+// has dropped 100-fold and before it stops; COCG-rq runs its recursion to
+// kInnerFrac * tol.  Then the true residual M^-1 (B - A X) decides; if it is
+// not below tol the solver restarts from the current X (warm start).  A
+// BiCGSTAB recursion that diverges under the complex64 products is abandoned
+// and the problem solved again with complex128 products.
+constexpr double kInnerFrac = 0.5;
+
+struct MLayout {
+  Layout base;
+  size_t in32, out32, diag32, jpre32, total;
+};
+
+static MLayout mlayout(const bdda_plan* p, int L, int n_occ) {
+  MLayout o;
+  o.base = layout(p, BDDA_C128, L, n_occ);
+  const size_t v32 = (size_t)3 * n_occ * L * 8;
+  size_t off = o.base.total;
+  o.in32 = off; off = al(off + v32);
+  o.out32 = off; off = al(off + v32);
+  o.diag32 = off; off = al(off + (size_t)3 * n_occ * 8);
+  o.jpre32 = off; off = al(off + (size_t)3 * n_occ * 8);
+  o.total = off;
+  return o;
+}
+
+static int run_mixed(int solver, const bdda_plan* p, int L, int n_occ, const void* ghat64, const void* ghat32,
+                     const int32_t* cell_map, const double2* diag, const double2* B, const double2* X0, double tol,
+                     int itermax, int max_outer, double2* Xout, int* iter_fin, double* err_fin, double* hist,
+                     void* work, size_t work_bytes, cudaStream_t st) {
+  const MLayout o = mlayout(p, L, n_occ);
+  if (work_bytes < o.total) return BDDA_NO_WORKSPACE;
+  unsigned char* w = static_cast<unsigned char*>(work);
+  Ctx<double2> c;
+  fill_ctx(c, p, L, n_occ, ghat64, cell_map, w, o.base.field, o.base.diag, o.base.jpre, o.base.vec, kVecs,
+           o.base.partial, o.base.small, o.base.state, st);
+  TRY(allow_smem(bicg_alpha_kernel, c.sm2));
+  TRY(allow_smem(bicg_zeta_beta_kernel, c.sm2));
+  TRY(allow_smem(cholqr_step_kernel, c.sm2));
+  TRY(allow_smem(cocg_alpha_kernel, c.sm3));
+  TRY(allow_smem(cocg_xi_kernel, c.sm3));
+  TRY(allow_smem(cocg_beta_kernel, c.sm3));
+  float2* in32 = reinterpret_cast<float2*>(w + o.in32);
+  float2* out32 = reinterpret_cast<float2*>(w + o.out32);
+  float2* diag32 = reinterpret_cast<float2*>(w + o.diag32);
+  float2* jpre32 = reinterpret_cast<float2*>(w + o.jpre32);
+  const int64_t ne = c.n * L;
+  // vec: 0 X, 1 R, 4 V, 7 Bj (the solver cores' roles)
+  double2 *X = c.vec[0], *R = c.vec[1], *V = c.vec[4], *Bj = c.vec[7];
+  BDDA_CUDA_TRY(cudaMemsetAsync(c.st, 0, sizeof(SolverState), st));
+  constants_kernel<<<1, 32, 0, st>>>(c.sp);
+  prepare_kernel<double2><<<kRedBlocks, 256, 0, st>>>(diag, B, c.n, L, c.diag, c.jpre, Bj);
+  prepare_kernel<float2><<<kRedBlocks, 256, 0, st>>>(diag, B, c.n, L, diag32, jpre32, in32);
+  count_launch(3);
+  BDDA_CUDA_TRY(cudaGetLastError());
+  if (X0) BDDA_CUDA_TRY(cudaMemcpyAsync(X, X0, (size_t)ne * sizeof(double2), cudaMemcpyDeviceToDevice, st));
+  else BDDA_CUDA_TRY(cudaMemsetAsync(X, 0, (size_t)ne * sizeof(double2), st));
+  int total = 0;
+  *iter_fin = 0;
+  *err_fin = INFINITY;
+  int status = BDDA_NOT_CONVERGED;
+  double prev = INFINITY;
+  for (int round = 0; round < max_outer && total < itermax; ++round) {
+    c.ghat32 = static_cast<const float2*>(ghat32);
+    c.diag32 = diag32;
+    c.jpre32 = jpre32;
+    c.in32 = in32;
+    c.out32 = out32;
+    int it_in = 0;
+    double err_in = INFINITY;
+    const bool warm = round > 0 || X0 != nullptr;
+    // BiCGSTAB judges convergence on a replaced (true) residual; COCG-rq's
+    // residual is implicit, so its recursion runs to kInnerFrac * tol
+    const int s_in = solver == BDDA_COCG_RQ
+                         ? cocg_core<double2>(c, warm, kInnerFrac * tol, itermax - total, &it_in, &err_in,
+                                              hist ? hist + total : nullptr)
+                         : bicgstab_core<double2>(c, warm, tol, itermax - total, &it_in, &err_in,
+                                                  hist ? hist + total : nullptr);
+    if (s_in != BDDA_OK && s_in != BDDA_NOT_CONVERGED) return s_in;
+    total += it_in + 1;
+    *iter_fin = total - 1;
+    if (c.diverged) {   // give up the complex64 products: complex128 from the start
+      c.diverged = false;
+      c.ghat32 = nullptr;
+      if (X0) BDDA_CUDA_TRY(cudaMemcpyAsync(X, X0, (size_t)ne * sizeof(double2), cudaMemcpyDeviceToDevice, st));
+      else BDDA_CUDA_TRY(cudaMemsetAsync(X, 0, (size_t)ne * sizeof(double2), st));
+      if (total < itermax) {
+        const int s64 = bicgstab_core<double2>(c, X0 != nullptr, tol, itermax - total, &it_in, &err_in,
+                                               hist ? hist + total : nullptr);
+        if (s64 != BDDA_OK && s64 != BDDA_NOT_CONVERGED) return s64;
+        total += it_in + 1;
+        *iter_fin = total - 1;
+      }
+      max_outer = round + 1;   // this is the last round
+    }
+    // true residual with the complex128 product
+    c.ghat32 = nullptr;
+    TRY(mvp_exact<double2>(c, X, V));
+    TRY(upd<double2>(c, R, Bj, nullptr, V, c.sp.r, nullptr, nullptr, nullptr, nullptr, true));
+    norm_kernel<<<1, 256, 0, st>>>(reinterpret_cast<double*>(c.partial), kRedBlocks, c.st, 0);
+    count_launch();
+    double err = INFINITY;
+    int bad = 0;
+    TRY(read_state(c, &err, &bad));
+    *err_fin = err;
+    if (bad == 2 || !(err == err)) break;
+    if (err < tol) { status = BDDA_OK; break; }
+    if (!(err < 0.9 * prev)) break;   // restarts no longer gain
+    prev = err;
+  }
+  BDDA_CUDA_TRY(cudaMemcpyAsync(Xout, X, (size_t)ne * sizeof(double2), cudaMemcpyDeviceToDevice, st));
+  return status;
+}
+
 }  // namespace bdda
 
 using namespace bdda;
@@ -832,5 +1007,24 @@ int bdda_refine_solve(const bdda_plan* p, int solver, int L, int n_occ, const vo
                     (cudaStream_t)stream);
 }
 
-}  // extern "C"
+size_t bdda_mixed_workspace_bytes(const bdda_plan* p, int L, int n_occ) {
+  if (!p || L < 1 || L > kMaxL || n_occ < 1) return 0;
+  return mlayout(p, L, n_occ).total;
+}
 
+int bdda_mixed_solve(const bdda_plan* p, int solver, int L, int n_occ, const void* ghat_c128, const void* ghat_c64,
+                     const int32_t* cell_map, const void* diag, const void* B, const void* X0, double tol,
+                     int itermax, int max_outer, void* X, int* iter_fin, double* err_fin, double* history,
+                     void* work, size_t work_bytes, void* stream) {
+  if (!p || L < 1 || L > kMaxL || n_occ < 1 || !ghat_c128 || !ghat_c64 || !cell_map || !diag || !B || !X ||
+      !iter_fin || !err_fin || itermax < 0 || !(tol > 0.0) || max_outer < 1 ||
+      (solver != BDDA_BICGSTAB && solver != BDDA_COCG_RQ))
+    return BDDA_BAD_ARG;
+  if (!p->dev_tables || !work) return BDDA_NO_WORKSPACE;
+  return run_mixed(solver, p, L, n_occ, ghat_c128, ghat_c64, cell_map, static_cast<const double2*>(diag),
+                   static_cast<const double2*>(B), static_cast<const double2*>(X0), tol, itermax, max_outer,
+                   static_cast<double2*>(X), iter_fin, err_fin, history, work, work_bytes,
+                   static_cast<cudaStream_t>(stream));
+}
+
+}  // extern "C"

@@ -221,6 +221,62 @@ int bdda_refine_solve(const bdda_plan* plan, int solver, int L, int n_occ, const
                       int* iter_fin, double* err_fin, double* history, void* work, size_t work_bytes,
                       void* stream);
 
+/* ---- complex128 Krylov with complex64 products (no counterpart in the
+ * reference) ------------------------------------------------------------------
+ * The block solver of `solver` with X, the residual, every Krylov vector,
+ * Gram product and L x L step in complex128, and the products inside the
+ * iteration in complex64 (ghat_c64 from bdda_green_convert).  The recursion
+ * runs to tol / 2; the true residual ||M^-1 (B - A X)|| / ||M^-1 B|| from the
+ * complex128 product then decides, and the solver restarts from X (exact
+ * product) while it is not below tol, up to max_outer rounds.  err_fin is
+ * that true residual; iter_fin counts the iterations of all rounds. */
+size_t bdda_mixed_workspace_bytes(const bdda_plan* plan, int L, int n_occ);
+int bdda_mixed_solve(const bdda_plan* plan, int solver, int L, int n_occ, const void* ghat_c128,
+                     const void* ghat_c64, const int32_t* cell_map, const void* diag, const void* B,
+                     const void* X0, double tol, int itermax, int max_outer, void* X, int* iter_fin,
+                     double* err_fin, double* history, void* work, size_t work_bytes, void* stream);
+
+/* ---- batched solve (no counterpart in the reference, which solves one problem
+ * per call: scatterer.py:169-171 inside the loops of run_dda.py:56-65) --------
+ * Many independent block-BiCGSTAB problems -- particles, wavelengths,
+ * orientation blocks, each with its own plan (grid), Green's spectrum,
+ * occupancy map, Jacobi diagonal and right-hand sides -- advance together:
+ * every step of an iteration is one persistent launch over a device work list
+ * of the problems still iterating, each problem's convergence test runs on
+ * the device, and the iteration is replayed as a CUDA graph (use_graph != 0).
+ * Per problem the result is that of bdda_bicgstab (mode C128 / C64) or of
+ * bdda_mixed_solve (mode MIXED, at most max_outer rounds).  All problems share L, which
+ * is 8, 16, 32 or 64; at most 1024 problems per call. */
+typedef struct bdda_batch_problem {
+  const bdda_plan* plan;      /* the problem's grid, tables attached */
+  int n_occ;                  /* occupied dipoles */
+  const void* ghat;           /* complex128 spectrum (modes C128 and MIXED) */
+  const void* ghat_c64;       /* complex64 spectrum (modes C64 and MIXED) */
+  const int32_t* cell_map;    /* bdda_occupancy_map of the problem */
+  const void* diag;           /* complex128 [3 n_occ], DIAG_A */
+  const void* B;              /* complex128 [3 n_occ][L] */
+  const void* X0;             /* complex128 [3 n_occ][L] warm start, or NULL */
+  void* X;                    /* complex128 [3 n_occ][L] output */
+} bdda_batch_problem;
+
+enum bdda_batch_mode {
+  BDDA_BATCH_C128 = 0,        /* complex128 solves */
+  BDDA_BATCH_C64 = 1,         /* complex64 vectors and products, FP64 Gram / L x L */
+  BDDA_BATCH_MIXED = 2        /* complex128 vectors, complex64 products (bdda_mixed_solve) */
+};
+
+/* Device workspace of one batched call (0: bad arguments). */
+size_t bdda_batch_workspace_bytes(const bdda_batch_problem* problems, int nprob, int mode, int L, int itermax);
+/* status[i], iter_fin[i], err_fin[i] (host arrays of nprob) receive each
+ * problem's outcome as bdda_bicgstab reports it; history (host, nprob x
+ * itermax, nullable) the residual per iteration.  Returns BDDA_OK when every
+ * problem converged, else BDDA_BREAKDOWN if one broke down, else
+ * BDDA_NOT_CONVERGED; argument and CUDA errors as elsewhere.  Runs on its own
+ * stream ordered after `stream`, and synchronises it. */
+int bdda_batch_bicgstab(const bdda_batch_problem* problems, int nprob, int mode, int L, double tol, int itermax,
+                        int max_outer, int use_graph, int* status, int* iter_fin, double* err_fin, double* history,
+                        void* work, size_t work_bytes, void* stream);
+
 /* ---- physics around the solve --------------------------------------------------
  * Homogeneous particle, per-axis index m_p_xyz = (re x, im x, re y, im y, re z, im z):
  * eps_r = m_p^2 / m_m^2, Clausius-Mossotti polarizability with the CR2009

@@ -94,3 +94,37 @@ def test_plan_accepts_explicit_grid_and_rejects_short_or_rough():
     assert _plan((5, 4, 6), (8, 10, 15))[0] == _lib.BAD_ARG     # 8 < 2*5-1
     assert _plan((5, 4, 6), (11, 10, 15))[0] == _lib.BAD_ARG    # 11 is not 7-smooth
     assert _plan((0, 4, 6))[0] == _lib.BAD_ARG
+
+
+def test_batch_workspace_query_checks_arguments():
+    """Host-only: the batched solver's workspace query accepts valid work lists and rejects bad ones."""
+    import ctypes as C
+    import sys
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), "..", "block-dda_py_b200"))
+    from bl_krylov.bl_krylov import _BatchProblem
+    lib = _lib.load()
+    plans = []
+    for n in ((8, 7, 6), (17, 17, 17)):
+        h = C.c_void_p()
+        assert lib.bdda_plan_create((C.c_int * 3)(*n), None, C.byref(h)) == 0
+        plans.append(h)
+    arr = (_BatchProblem * 2)()
+    for i, h in enumerate(plans):
+        s = arr[i]
+        s.plan = h.value
+        s.n_occ = 100 * (i + 1)
+        s.ghat = s.ghat_c64 = s.cell_map = s.diag = s.B = s.X = 256   # never dereferenced by the query
+    try:
+        b8 = lib.bdda_batch_workspace_bytes(arr, 2, _lib.BATCH_MIXED, 8, 50)
+        b64 = lib.bdda_batch_workspace_bytes(arr, 2, _lib.BATCH_MIXED, 64, 50)
+        assert 0 < b8 < b64
+        assert lib.bdda_batch_workspace_bytes(arr, 2, _lib.BATCH_C64, 8, 50) < b8
+        assert lib.bdda_batch_workspace_bytes(arr, 2, _lib.BATCH_MIXED, 12, 50) == 0   # L not 8/16/32/64
+        assert lib.bdda_batch_workspace_bytes(arr, 0, _lib.BATCH_MIXED, 8, 50) == 0
+        assert lib.bdda_batch_workspace_bytes(arr, 2, 3, 8, 50) == 0
+        arr[1].ghat_c64 = None
+        assert lib.bdda_batch_workspace_bytes(arr, 2, _lib.BATCH_MIXED, 8, 50) == 0   # spectrum missing
+        assert lib.bdda_batch_workspace_bytes(arr, 2, _lib.BATCH_C128, 8, 50) > 0
+    finally:
+        for h in plans:
+            lib.bdda_plan_destroy(h)

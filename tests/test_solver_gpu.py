@@ -181,17 +181,19 @@ def test_specialised_block_kernels_match_generic(mods, L, solver):
     assert rel(X1, X2) < 1e-5
 
 
+@pytest.mark.parametrize("precision", ["mixed", "mixed-fp32"])
 @pytest.mark.parametrize("solver", ["bicgstab", "cocg"])
-def test_mixed_precision_refinement_meets_fp64_accuracy(mods, solver):
-    """FP32 block solves inside FP64 refinement reach the true residual 1e-5 and
-    the observables agree with the FP64 solve within 1e-4 (the metric's bound)."""
+def test_mixed_precision_refinement_meets_fp64_accuracy(mods, solver, precision):
+    """Both mixed forms (complex64 products in complex128 Krylov; complex64
+    block solves inside FP64 refinement) reach the true residual 1e-5 and the
+    observables agree with the FP64 solve within 1e-4 (the metric's bound)."""
     mf, bk = mods
     rec = load_geometry(os.path.join(GOLDEN, "geometry_cfg1.npz"))
     n, lf, address, pos, geom, eper_r, diag, B = _case(rec)
     til = mf.fft_init(n, 3, lf, geom["k"])
     fn = solver_fn(bk, solver)
     hist = []
-    Xm, itm, errm = fn(n, 3, address, til, diag, B, 1e-5, 400, precision="mixed", history=hist)
+    Xm, itm, errm = fn(n, 3, address, til, diag, B, 1e-5, 400, precision=precision, history=hist)
     assert errm < 1e-5 and len(hist) == itm + 1
     true = O.true_residual(n, 3, address, O.fft_init(n, 3, lf, geom["k"]), diag, B, Xm)
     assert abs(true - errm) < 1e-3 * errm + 1e-9      # err_fin is the true residual
@@ -213,3 +215,28 @@ def test_reliable_update_variant_small_block(mods):
     true = O.true_residual(n, 3, address, O.fft_init(n, 3, lf, geom["k"]), diag, B, X)
     assert abs(true - err) < 1e-3 * err + 1e-9
     assert it + 1 <= 2 * (int(rec["bicgstab_tol5_iter_fin"]) + 1)
+
+
+def test_mixed_form_converges_where_fp32_krylov_diverges(mods):
+    """A strongly scattering GRE (x = 9.2, m = 1.53 + 0.005i, 34 x 65 x 69
+    lattice): complex64 Krylov vectors diverge here, the mixed form (complex64
+    products only) converges like complex128 and gives its observables."""
+    from bdda_b200.inputs import so3_euler
+    from bdda_b200.shapes import gre_particle
+    mf, bk = mods
+    g = gre_particle(9.197523282837686, 0.6459893079939255, 0.7681224627849057, 0.04502319853187231, seed=3005,
+                     wl_0=0.55)
+    rec = dict(g, euler=so3_euler(8, 16), m_p_xyz=np.array([1.53 + 0.005j] * 3))
+    n, lf, address, pos, geom, eper_r, diag, B = _case(rec)
+    til = mf.fft_init(n, 3, lf, geom["k"])
+    X64, it64, err64 = bk.bl_bicgstab_jacobi_mvp_fft(n, 3, address, til, diag, B, 1e-5, 400)
+    Xm, itm, errm = bk.bl_bicgstab_jacobi_mvp_fft(n, 3, address, til, diag, B, 1e-5, 400, precision="mixed")
+    Xc, _, errc = bk.bl_bicgstab_jacobi_mvp_fft(n, 3, address, til, diag, B, 1e-10, 600)
+    assert err64 < 1e-5 and errm < 1e-5 and errc < 1e-10
+    assert itm <= 1.25 * it64 + 5
+    o64 = O.observables(X64, geom, pos, eper_r, lf)
+    om = O.observables(Xm, geom, pos, eper_r, lf)
+    oc = O.observables(Xc, geom, pos, eper_r, lf)
+    # against the converged solution the mixed form is as accurate as complex128 at the same tolerance
+    for key in ("C_ext", "S_fw_theta", "S_fw_phi", "S_bk"):
+        assert rel(om[key], oc[key]) < max(3 * rel(o64[key], oc[key]), 1e-5), key
