@@ -525,6 +525,93 @@ def run_sweep(args):
     print(json.dumps(out), flush=True)
 
 
+# ---------------------------------------------------------------------------
+# learned warm start: train on solver solutions, evaluate on held-out particles
+# ---------------------------------------------------------------------------
+def _fno_shape(spec):
+    from bdda_b200.warmstart import _shape
+    return _shape(spec)
+
+
+def run_fno(args):
+    """Train the FNO warm start on GPU-solved GRE particles and compare, on
+    held-out particles, iterations and time to 1e-5 from zero and from the
+    warm start (complex128 block-BiCGSTAB), with the fallback rate."""
+    import concurrent.futures
+    import multiprocessing
+    from bdda_b200.warmstart import sample_particles
+    L = 16
+    train_specs = sample_particles(args.fno_train, seed=4)
+    eval_specs = sample_particles(args.fno_eval, seed=40)
+    for var in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS"):
+        os.environ[var] = "1"
+    t0 = time.perf_counter()
+    with concurrent.futures.ProcessPoolExecutor(max_workers=max(1, min(32, (os.cpu_count() or 2) - 1)),
+                                                mp_context=multiprocessing.get_context("spawn")) as ex:
+        shapes = list(ex.map(_fno_shape, train_specs + eval_specs))
+    shape_s = time.perf_counter() - t0
+    import torch
+    from bdda_b200.warmstart import WarmStartFNO, make_dataset
+    from bl_krylov import bl_krylov as bk
+    t0 = time.perf_counter()
+    train = make_dataset(train_specs, L=L, shapes=shapes[:len(train_specs)])
+    torch.cuda.synchronize()
+    data_s = time.perf_counter() - t0
+    for d in train:   # training needs no Green's spectrum
+        d.pop("green", None)
+    model = WarmStartFNO(layers=4, modes=args.fno_modes, seed=4)
+    t0 = time.perf_counter()
+    losses = model.fit(train, epochs=args.fno_epochs, lr=args.fno_lr, lr_final=args.fno_lr * 0.05, seed=4)
+    torch.cuda.synchronize()
+    train_s = time.perf_counter() - t0
+    if args.fno_save:
+        model.save(args.fno_save)
+    del train
+    evald = make_dataset(eval_specs, L=L, shapes=shapes[len(train_specs):])
+    rows = []
+    for d in evald:
+        args_ = (d["n"], 3, d["occ"], d["green"], d["diag"], d["B"], TOL, ITERMAX)
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        _, it0, e0 = bk.bl_bicgstab_jacobi_mvp_fft(*args_)
+        torch.cuda.synchronize()
+        t_zero = time.perf_counter() - t
+        t = time.perf_counter()
+        X0, nfb = model.warm_start(d["n"], d["occ"], d["green"], d["diag"], d["B"], d["eps_r"])
+        torch.cuda.synchronize()
+        t_inf = time.perf_counter() - t
+        hist = []
+        _, it1, e1 = bk.bl_bicgstab_jacobi_mvp_fft(*args_, X0=X0, history=hist)
+        torch.cuda.synchronize()
+        t_warm = time.perf_counter() - t
+        rows.append(dict(n=list(d["n"]), iters_zero=it0 + 1, iters_warm=it1 + 1, ok=bool(e0 < TOL and e1 < TOL),
+                         fallback_cols=nfb, t_zero=t_zero, t_warm=t_warm, t_infer=t_inf,
+                         r0_warm=hist[0] if hist else None))
+    iz = np.array([r["iters_zero"] for r in rows], float)
+    iw = np.array([r["iters_warm"] for r in rows], float)
+    tz = sum(r["t_zero"] for r in rows)
+    tw = sum(r["t_warm"] for r in rows)
+    out = {"metric": "learned warm start: iterations and time to rel-res 1e-5, zero vs FNO initial guess",
+           "config": {"workload": "GRE x~U[4,12], ab,bc~U[0.5,1], beta~U[0,0.2], Re m_p~U[1.3,1.7], Im~U[0,0.1], "
+                                  "birefringence +-0.05 (seed 4 train / 40 held out), lambda/16, L=%d, complex128 "
+                                  "block-BiCGSTAB" % L,
+                      "fno": {"layers": 4, "width": 32, "modes": args.fno_modes, "params": model.n_params,
+                              "weights": "FP32", "accumulation": "FP32"},
+                      "train_particles": args.fno_train, "train_samples": args.fno_train * L,
+                      "eval_particles": len(rows), "epochs": args.fno_epochs},
+           "eval": {"iterations_zero_mean": round(float(iz.mean()), 2), "iterations_warm_mean": round(float(iw.mean()), 2),
+                    "iterations_saved_frac": round(float(1 - iw.sum() / iz.sum()), 4),
+                    "time_zero_s": round(tz, 3), "time_warm_s_incl_inference": round(tw, 3),
+                    "speedup": round(tz / tw, 3),
+                    "fallback_rate_columns": round(sum(r["fallback_cols"] for r in rows) / (L * len(rows)), 4),
+                    "all_converged": all(r["ok"] for r in rows)},
+           "train": {"loss_first_epoch": round(losses[0], 4), "loss_last_epoch": round(losses[-1], 4),
+                     "seconds": round(train_s, 2), "data_generation_s": round(data_s, 2),
+                     "shapes_host_s": round(shape_s, 2)},
+           "per_particle": rows if args.fno_verbose else None}
+    print(json.dumps(out), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -540,7 +627,18 @@ def main():
     ap.add_argument("--sweep", action="store_true",
                     help="batched uneven sweep (48 GRE particles x 3 wavelengths, L=32) instead of the headline")
     ap.add_argument("--sweep-particles", type=int, default=48)
+    ap.add_argument("--fno", action="store_true", help="train and evaluate the learned warm start")
+    ap.add_argument("--fno-train", type=int, default=256)
+    ap.add_argument("--fno-eval", type=int, default=32)
+    ap.add_argument("--fno-epochs", type=int, default=20)
+    ap.add_argument("--fno-modes", type=int, default=12)
+    ap.add_argument("--fno-lr", type=float, default=2e-3)
+    ap.add_argument("--fno-save", default=None)
+    ap.add_argument("--fno-verbose", action="store_true")
     args = ap.parse_args()
+    if args.fno:
+        run_fno(args)
+        return
     if args.sweep:
         run_sweep(args)
         return

@@ -41,6 +41,16 @@ PROTOTYPES = {
     "bdda_tune_pass": (_i, [_i, _i, _i, _i, _i, _i]),
     "bdda_batch_workspace_bytes": (_sz, [_vp, _i, _i, _i, _i]),
     "bdda_mixed_workspace_bytes": (_sz, [_vp, _i, _i]),
+    "bdda_fno_param_count": (_sz, [_vp]),
+    "bdda_fno_offset": (_sz, [_vp, _i, _i]),
+    "bdda_fno_workspace_bytes": (_sz, [_vp, _i, _pi]),
+    "bdda_fno_buffer_offset": (_sz, [_vp, _i, _pi, _i]),
+    "bdda_fno_features": (_i, [_vp, _pi, _i, _i, _vp, _vp, _vp, _pd, _vp, _vp, _sz, _vp]),
+    "bdda_fno_forward": (_i, [_vp, _i, _pi, _vp, _i, _vp, _sz, _vp]),
+    "bdda_fno_loss": (_i, [_vp, _i, _pi, _i, _vp, _vp, _vp, _vp, _vp, _pd, _vp, _sz, _vp]),
+    "bdda_fno_backward": (_i, [_vp, _i, _pi, _vp, _vp, _vp, _vp, _sz, _vp]),
+    "bdda_fno_adam": (_i, [_vp, _vp, _vp, _vp, _sz, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float, _i, _vp]),
+    "bdda_fno_warm_start": (_i, [_vp, _pi, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _sz, _vp]),
     "bdda_mixed_solve": (_i, [_vp, _i, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _d, _i, _i, _vp, _pi, _pd, _pd,
                               _vp, _sz, _vp]),
     "bdda_batch_bicgstab": (_i, [_vp, _i, _i, _i, _d, _i, _i, _i, _pi, _pi, _pd, _pd, _vp, _sz, _vp]),

@@ -277,6 +277,60 @@ int bdda_batch_bicgstab(const bdda_batch_problem* problems, int nprob, int mode,
                         int max_outer, int use_graph, int* status, int* iter_fin, double* err_fin, double* history,
                         void* work, size_t work_bytes, void* stream);
 
+/* ---- learned warm start (no counterpart in the reference, whose solvers
+ * start from X0 = 0: bl_krylov.py:84-85,146) ------------------------------------
+ * A Fourier neural operator maps, per lattice cell and orientation, the
+ * occupancy mask, the per-axis chi = (eps - 1)/(eps + 2) and the Jacobi guess
+ * J = B / DIAG_A (scaled by its RMS) to a correction of J:
+ * X0 = J + scale * y.  lift cin -> width, `layers` Fourier layers (per-mode
+ * complex width x width matrices on the `modes` lowest frequencies per axis,
+ * plus a pointwise width x width map, GELU), projection width -> proj -> cout.
+ * The shipped shapes are cin 13, width 32, cout 6, proj 64; every lattice
+ * axis is at least `modes` and at most 128 cells.  One call handles B samples
+ * (orientations) of one lattice; activations live in `work`
+ * (bdda_fno_workspace_bytes), parameters in one FP32 array
+ * (bdda_fno_param_count floats, layout by bdda_fno_offset).  bdda_fno_features
+ * also writes the lattice's DFT tables into `work`; the other calls on that
+ * workspace use them, so it comes first for each lattice. */
+typedef struct bdda_fno_config {
+  int cin, width, cout, proj, layers, modes;
+} bdda_fno_config;
+
+size_t bdda_fno_param_count(const bdda_fno_config* cfg);
+/* what: 0 P, 1 p, 2 R_l, 3 W_l, 4 b_l, 5 Q1, 6 q1, 7 Q2, 8 q2 (float offset) */
+size_t bdda_fno_offset(const bdda_fno_config* cfg, int what, int layer);
+size_t bdda_fno_workspace_bytes(const bdda_fno_config* cfg, int B, const int n[3]);
+/* byte offset in `work` of: 0 features [B][cells][cin], 1 output [B][cells][cout],
+ * 2 mask [cells], 3 loss gradient [B][cells][cout], 4 target [B][cells][cout] */
+size_t bdda_fno_buffer_offset(const bdda_fno_config* cfg, int B, const int n[3], int which);
+/* Features of the L = B orientations of one particle into work; scale (device,
+ * L doubles) receives the RMS of each Jacobi-guess column. */
+int bdda_fno_features(const bdda_fno_config* cfg, const int n[3], int n_occ, int L, const int32_t* cell_map,
+                      const void* diag, const void* B, const double chi[6], double* scale, void* work,
+                      size_t work_bytes, void* stream);
+/* Forward pass on the features in work (train != 0 keeps what backward needs). */
+int bdda_fno_forward(const bdda_fno_config* cfg, int B, const int n[3], const float* params, int train, void* work,
+                     size_t work_bytes, void* stream);
+/* Masked relative squared error of the output against the solution X
+ * (complex128 [3 n_occ][B]): mean over samples of
+ * sum |y - (X - J)/scale|^2 / sum |(X - J)/scale|^2 over occupied cells; its
+ * gradient w.r.t. the output goes to the work buffer 3.  *loss is written
+ * when the stream reaches it. */
+int bdda_fno_loss(const bdda_fno_config* cfg, int B, const int n[3], int n_occ, const int32_t* cell_map,
+                  const void* diag, const void* Bm, const void* X, const double* scale, double* loss, void* work,
+                  size_t work_bytes, void* stream);
+/* Gradients of every parameter, ADDED to grads (zero it first); grad_out null
+ * means the loss gradient in work. */
+int bdda_fno_backward(const bdda_fno_config* cfg, int B, const int n[3], const float* params, const float* grad_out,
+                      float* grads, void* work, size_t work_bytes, void* stream);
+/* One Adam step (bias-corrected, decoupled weight decay as L2 on the gradient). */
+int bdda_fno_adam(float* params, const float* grads, float* m, float* v, size_t n, float lr, float beta1, float beta2,
+                  float eps, float weight_decay, int step, void* stream);
+/* X0 (complex128 [3 n_occ][L]) = J + scale * output at the occupied cells. */
+int bdda_fno_warm_start(const bdda_fno_config* cfg, const int n[3], int n_occ, int L, const int32_t* cell_map,
+                        const void* diag, const void* B, const double* scale, void* X0, void* work,
+                        size_t work_bytes, void* stream);
+
 /* ---- physics around the solve --------------------------------------------------
  * Homogeneous particle, per-axis index m_p_xyz = (re x, im x, re y, im y, re z, im z):
  * eps_r = m_p^2 / m_m^2, Clausius-Mossotti polarizability with the CR2009

@@ -1,0 +1,102 @@
+"""Learned warm start: the hand-written FNO kernels against the float64 CPU
+oracle (features, forward output, loss, and the gradient of every parameter
+block), and the warm start with its fallback rule."""
+import ctypes as C
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import fno_oracle as F
+
+pytestmark = pytest.mark.gpu
+
+
+def _rel(a, b):
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-30))
+
+
+@pytest.fixture(scope="module")
+def small():
+    """A 12 x 13 x 14 lattice, 60 % occupied, L = 3 orientations, random data."""
+    from bdda_b200.runtime import Occupancy, Plan
+    rng = np.random.default_rng(11)
+    n = (12, 13, 14)
+    ncell = int(np.prod(n))
+    address = np.sort(rng.choice(ncell, int(0.6 * ncell), replace=False))
+    n_occ = address.size
+    L = 3
+    diag = (rng.uniform(2, 5, 3 * n_occ) + 1j * rng.uniform(-1, 1, 3 * n_occ))
+    B = rng.standard_normal((3 * n_occ, L)) + 1j * rng.standard_normal((3 * n_occ, L))
+    X = B / diag[:, None] * (1 + 0.3 * rng.standard_normal((3 * n_occ, L)))
+    eps = np.array([2.3 + 0.1j, 2.5 + 0.05j, 2.1 + 0.2j])
+    plan = Plan(n)
+    occ = Occupancy(plan, address)
+    cell_map = np.full(ncell, -1, np.int64)
+    cell_map[address] = np.arange(n_occ)
+    return dict(n=n, L=L, n_occ=n_occ, diag=diag, B=B, X=X, eps=eps, occ=occ, cell_map=cell_map, rng=rng)
+
+
+def test_fno_kernels_match_cpu_oracle(small):
+    from bdda_b200.warmstart import WarmStartFNO, chi_of
+    s = small
+    layers, modes = 2, 4
+    model = WarmStartFNO(layers=layers, modes=modes, seed=3)
+    # random (not just initial) parameters so every path carries signal
+    g = torch.Generator(device="cpu").manual_seed(5)
+    model.params.copy_((torch.randn(model.n_params, generator=g) * 0.15).to(model.device))
+    dev = model.device
+    diag = torch.as_tensor(s["diag"], device=dev)
+    B = torch.as_tensor(s["B"], device=dev)
+    X = torch.as_tensor(s["X"], device=dev)
+    n, L, ncell = s["n"], s["L"], int(np.prod(s["n"]))
+    loss_gpu = model.loss_and_grad(n, s["occ"], diag, B, s["eps"], X)
+    work = model._workspace(L, n)
+    x_gpu = model.buffer(work, L, n, 0, L * ncell * 13).cpu().numpy().reshape(L, ncell, 13)
+    y_gpu = model.buffer(work, L, n, 1, L * ncell * 6).cpu().numpy().reshape(L, ncell, 6)
+    # features
+    x_ref, scale, J = F.features(s["cell_map"], s["n_occ"], s["diag"], s["B"], chi_of(s["eps"]))
+    assert _rel(x_gpu, x_ref) < 1e-6
+    # forward on the same (FP32) features, loss, gradients
+    params = F.unflatten(model.params.cpu().numpy(), layers, modes)
+    xt = torch.tensor(x_gpu.astype(np.float64).reshape((L,) + tuple(n) + (13,)))
+    y = F.forward(params, xt, n, layers, modes)
+    assert _rel(y_gpu.reshape(y.shape), y.detach().numpy()) < 1e-4
+    t = F.target(s["cell_map"], s["n_occ"], J, s["X"], scale).reshape((L,) + tuple(n) + (6,))
+    mask = torch.tensor((s["cell_map"] >= 0).reshape(n).astype(np.float64))
+    loss = F.loss(y, torch.tensor(t), mask)
+    assert abs(loss_gpu - loss.item()) < 1e-4 * loss.item()
+    loss.backward()
+    g_gpu = model.grads.cpu().numpy()
+    off = 0
+    for name, shape in F.param_layout(layers, modes):
+        k = int(np.prod(shape))
+        gr = params[name].grad.numpy().ravel()
+        assert _rel(g_gpu[off:off + k], gr) < 2e-3, name
+        off += k
+
+
+def test_warm_start_is_jacobi_plus_scaled_output_and_falls_back(small):
+    from bdda_b200.warmstart import WarmStartFNO
+    from mvp_fft import mvp_fft
+    s = small
+    model = WarmStartFNO(layers=2, modes=4, seed=1)
+    dev = model.device
+    diag = torch.as_tensor(s["diag"], device=dev)
+    B = torch.as_tensor(s["B"], device=dev)
+    X0 = model.predict(s["n"], s["occ"], diag, B, s["eps"]).cpu().numpy()
+    L, ncell = s["L"], int(np.prod(s["n"]))
+    work = model._workspace(L, s["n"])
+    y = model.buffer(work, L, s["n"], 1, L * ncell * 6).cpu().numpy().reshape(L, ncell, 6)
+    _, scale, J = F.features(s["cell_map"], s["n_occ"], s["diag"], s["B"], np.zeros(6))
+    occ = s["cell_map"] >= 0
+    yo = y[:, occ, :]                                   # (L, n_occ, 6) in dipole order
+    corr = (yo[..., 0::2] + 1j * yo[..., 1::2]).transpose(1, 2, 0).reshape(3 * s["n_occ"], L)
+    assert _rel(X0, J + corr * scale[None, :]) < 1e-6
+    # a column whose predicted initial residual exceeds ||M^-1 B|| starts from zero
+    green = mvp_fft.fft_init(s["n"], 3, 0.05, 2.0)
+    X0w, nfb = model.warm_start(s["n"], s["occ"], green, diag, B, s["eps"])
+    assert 0 <= nfb <= L
+    if X0w is not None:
+        zero_cols = (X0w.abs().sum(0) == 0).sum().item()
+        assert zero_cols == nfb
