@@ -559,6 +559,7 @@ def run_fno(args):
     data_s = time.perf_counter() - t0
     for d in train:   # training needs no Green's spectrum
         d.pop("green", None)
+    torch.cuda.empty_cache()
     model = WarmStartFNO(layers=4, modes=args.fno_modes, seed=4)
     t0 = time.perf_counter()
     losses = model.fit(train, epochs=args.fno_epochs, lr=args.fno_lr, lr_final=args.fno_lr * 0.05, seed=4)

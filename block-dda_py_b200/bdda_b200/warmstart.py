@@ -100,8 +100,9 @@ class WarmStartFNO:
             nb = int(_lib.load().bdda_fno_workspace_bytes(C.byref(self.cfg), int(L), _n3(n)))
             if nb == 0:
                 raise ValueError("bad FNO shape %r" % (key,))
-            if len(self._work) > 4:
+            if len(self._work) > 1:
                 self._work.clear()
+                torch.cuda.empty_cache()
             w = torch.empty(nb, dtype=torch.uint8, device=self.device)
             self._work[key] = w
         return w
@@ -130,32 +131,52 @@ class WarmStartFNO:
                                                 1 if train else 0, ptr(work), work.numel(),
                                                 stream_ptr(self.device)), "bdda_fno_forward")
 
+    # samples (orientations) per call: activations of at most max_rows lattice rows
+    max_rows = 4_000_000
+
+    def _chunks(self, n, L):
+        per = max(1, min(L, self.max_rows // int(np.prod([int(v) for v in n]))))
+        return [(c, min(L, c + per)) for c in range(0, L, per)]
+
     def predict(self, n, occ, diag, B, eps_r) -> torch.Tensor:
         """X0 = J + scale * FNO, complex128 (3 n_occ, L)."""
         L = int(B.shape[1])
-        work, scale = self.features(n, occ, diag, B, eps_r)
-        self.forward(work, L, n)
         X0 = torch.empty_like(B)
-        _lib.check(_lib.load().bdda_fno_warm_start(C.byref(self.cfg), _n3(n), occ.n_occ, L, ptr(occ.cell_map),
-                                                   ptr(diag), ptr(B), ptr(scale), ptr(X0), ptr(work), work.numel(),
-                                                   stream_ptr(self.device)), "bdda_fno_warm_start")
+        for c0, c1 in self._chunks(n, L):
+            Bc = B[:, c0:c1].contiguous()
+            work, scale = self.features(n, occ, diag, Bc, eps_r)
+            self.forward(work, c1 - c0, n)
+            Xc = torch.empty_like(Bc)
+            _lib.check(_lib.load().bdda_fno_warm_start(C.byref(self.cfg), _n3(n), occ.n_occ, c1 - c0,
+                                                       ptr(occ.cell_map), ptr(diag), ptr(Bc), ptr(scale), ptr(Xc),
+                                                       ptr(work), work.numel(), stream_ptr(self.device)),
+                       "bdda_fno_warm_start")
+            X0[:, c0:c1] = Xc
         return X0
 
     def loss_and_grad(self, n, occ, diag, B, eps_r, X) -> float:
-        """Forward, loss against the solution X and backward; gradients in self.grads."""
+        """Forward, loss against the solution X and backward over the orientations of
+        one particle, in chunks of orientations whose losses (each a mean over the
+        chunk) add; the summed gradient is in self.grads."""
         lib = _lib.load()
         L = int(B.shape[1])
-        work, scale = self.features(n, occ, diag, B, eps_r)
-        self.forward(work, L, n, train=True)
-        loss = C.c_double(0.0)
-        _lib.check(lib.bdda_fno_loss(C.byref(self.cfg), L, _n3(n), occ.n_occ, ptr(occ.cell_map), ptr(diag), ptr(B),
-                                     ptr(X), ptr(scale), C.byref(loss), ptr(work), work.numel(),
-                                     stream_ptr(self.device)), "bdda_fno_loss")
         self.grads.zero_()
-        _lib.check(lib.bdda_fno_backward(C.byref(self.cfg), L, _n3(n), ptr(self.params), None, ptr(self.grads),
-                                         ptr(work), work.numel(), stream_ptr(self.device)), "bdda_fno_backward")
-        torch.cuda.current_stream(self.device).synchronize()
-        return float(loss.value)
+        total = 0.0
+        for c0, c1 in self._chunks(n, L):
+            Bc = B[:, c0:c1].contiguous() if (c0, c1) != (0, L) else B
+            Xc = X[:, c0:c1].contiguous() if (c0, c1) != (0, L) else X
+            b = c1 - c0
+            work, scale = self.features(n, occ, diag, Bc, eps_r)
+            self.forward(work, b, n, train=True)
+            loss = C.c_double(0.0)
+            _lib.check(lib.bdda_fno_loss(C.byref(self.cfg), b, _n3(n), occ.n_occ, ptr(occ.cell_map), ptr(diag),
+                                         ptr(Bc), ptr(Xc), ptr(scale), C.byref(loss), ptr(work), work.numel(),
+                                         stream_ptr(self.device)), "bdda_fno_loss")
+            _lib.check(lib.bdda_fno_backward(C.byref(self.cfg), b, _n3(n), ptr(self.params), None, ptr(self.grads),
+                                             ptr(work), work.numel(), stream_ptr(self.device)), "bdda_fno_backward")
+            torch.cuda.current_stream(self.device).synchronize()
+            total += float(loss.value) * b / L
+        return total
 
     def adam(self, lr=1e-3, beta1=0.9, beta2=0.999, eps=1e-8, weight_decay=0.0):
         self.step += 1
@@ -255,6 +276,7 @@ def make_dataset(specs, L=16, tol=1e-5, itermax=600, shapes=None, max_cells=128,
         dds.append(d)
         keep.append(spec)
     sc.solve_matrix_equations(dds, precision="c128")
+    torch.cuda.empty_cache()
     data = []
     for spec, d in zip(keep, dds):
         eps = (np.asarray(spec["m_p"]) / 1.0) ** 2

@@ -272,7 +272,9 @@ def bl_bicgstab_jacobi_mvp_fft_batch(problems, tol, itermax, precision=None, max
     L = Ls.pop()
     itermax = int(itermax)
     dev = entries[0]["g"].plan.device
-    if max_bytes is None:
+    fixed_bound = max_bytes is not None
+    if not fixed_bound:
+        torch.cuda.empty_cache()
         free, _ = torch.cuda.mem_get_info(dev)
         max_bytes = int(0.7 * free)
     lib = _lib.load()
@@ -292,6 +294,7 @@ def bl_bicgstab_jacobi_mvp_fft_batch(problems, tol, itermax, precision=None, max
         if rc not in (0, 1, 2):
             _lib.check(rc, "bdda_batch_bicgstab")
         del work
+        torch.cuda.empty_cache()
         for i, e in enumerate(grp):
             s = int(st[i])
             X = None if s == 2 else (e["X"].cpu().numpy() if e["numpy"] else e["X"])
@@ -307,7 +310,8 @@ def bl_bicgstab_jacobi_mvp_fft_batch(problems, tol, itermax, precision=None, max
             sub_hist = [] if history is not None else None
             sub_st = []
             again = bl_bicgstab_jacobi_mvp_fft_batch([problems[i] for i in redo], tol, itermax, "c128",
-                                                     max_outer, graph, sub_hist, sub_st, max_bytes)
+                                                     max_outer, graph, sub_hist, sub_st,
+                                                     max_bytes if fixed_bound else None)
             for j, i in enumerate(redo):
                 X, it, er = again[j]
                 results[i] = (X, results[i][1] + 1 + it, er, sub_st[j])

@@ -107,17 +107,15 @@ __global__ void __launch_bounds__(kMaxBatch) list_kernel(ListDev l, const int* f
   }
 }
 
-__device__ __forceinline__ void list_find(const ListDev& l, int cls, int64_t item, int* p, int64_t* bid) {
-  const int n = l.ctl[0];
-  const int64_t* st = l.start + (int64_t)cls * (l.nprob + 1);
-  int lo = 0, hi = n - 1;   // largest k with st[k] <= item
+// Largest k in [lo, n) with st[k] <= item (st ascending, st[lo] <= item).
+__device__ __forceinline__ int list_search(const int64_t* st, int lo, int n, int64_t item) {
+  int hi = n - 1;
   while (lo < hi) {
     const int mid = (lo + hi + 1) >> 1;
     if (st[mid] <= item) lo = mid;
     else hi = mid - 1;
   }
-  *p = l.act[lo];
-  *bid = item - st[lo];
+  return lo;
 }
 
 // Copies one problem's argument struct into shared memory (all threads).
@@ -127,6 +125,45 @@ __device__ __forceinline__ void load_args(A* dst, const A* src) {
   const uint32_t* s = reinterpret_cast<const uint32_t*>(src);
   uint32_t* d = reinterpret_cast<uint32_t*>(dst);
   for (int i = threadIdx.x; i < (int)(sizeof(A) / 4); i += blockDim.x) d[i] = s[i];
+}
+
+// Walks this CTA's items of class cls (grid-stride, so every CTA sees every
+// problem and uneven problems balance).  Items arrive in increasing order, so
+// the CTA keeps a cursor into the list: it searches only when an item leaves
+// the current problem, and reloads the problem's arguments (into sargs) only
+// then.  body(p, bid) runs with all threads.
+template <typename ArgT, typename F>
+__device__ __forceinline__ void for_items(const ListDev& l, int cls, const ArgT* args, ArgT* sargs, F&& body) {
+  __shared__ int s_k, s_p, s_changed;
+  __shared__ int64_t s_base, s_end;
+  const int64_t total = l.total[cls];
+  const int n = l.ctl[0];
+  const int64_t* st = l.start + (int64_t)cls * (l.nprob + 1);
+  if (threadIdx.x == 0) {
+    s_k = 0;
+    s_p = -1;
+    s_end = -1;   // forces the first search
+  }
+  __syncthreads();
+  for (int64_t item = blockIdx.x; item < total; item += gridDim.x) {
+    if (threadIdx.x == 0) {
+      s_changed = 0;
+      if (item >= s_end) {
+        const int k = list_search(st, s_end < 0 ? 0 : s_k, n, item);
+        s_k = k;
+        s_base = st[k];
+        s_end = st[k + 1];
+        const int p = l.act[k];
+        s_changed = p != s_p;
+        s_p = p;
+      }
+    }
+    __syncthreads();
+    if (s_changed && args) load_args(sargs, args + s_p);
+    __syncthreads();
+    body(s_p, item - s_base);
+    __syncthreads();
+  }
 }
 
 // ---- per-problem device descriptor -----------------------------------------------
@@ -146,46 +183,15 @@ template <typename T, int KIND, int LT>
 __global__ void __launch_bounds__(256) batch_pencil_kernel(const PassArgs* args, ListDev l, int cls) {
   extern __shared__ __align__(16) unsigned char smraw[];
   __shared__ __align__(16) PassArgs sa;
-  __shared__ int sp;
-  __shared__ int64_t sbid;
-  const int64_t total = l.total[cls];
-  for (int64_t item = blockIdx.x; item < total; item += gridDim.x) {
-    if (threadIdx.x == 0) {
-      int p;
-      int64_t bid;
-      list_find(l, cls, item, &p, &bid);
-      sp = p;
-      sbid = bid;
-    }
-    __syncthreads();
-    load_args(&sa, args + sp);
-    __syncthreads();
-    generic_pencil<T, KIND, LT>(sa, sbid, smraw);
-    __syncthreads();
-  }
+  for_items(l, cls, args, &sa, [&](int, int64_t bid) { generic_pencil<T, KIND, LT>(sa, bid, smraw); });
 }
 
 template <typename T, bool CONJ, int L, int NB>
 __global__ void __launch_bounds__(256) batch_gram_kernel(const GramArgs* args, const ProbDev* pd, ListDev l) {
   extern __shared__ __align__(16) unsigned char smraw[];
   __shared__ __align__(16) GramArgs sg;
-  __shared__ int sp;
-  __shared__ int64_t sbid;
-  const int64_t total = l.total[kClsBlas];
-  for (int64_t item = blockIdx.x; item < total; item += gridDim.x) {
-    if (threadIdx.x == 0) {
-      int p;
-      int64_t bid;
-      list_find(l, kClsBlas, item, &p, &bid);
-      sp = p;
-      sbid = bid;
-    }
-    __syncthreads();
-    load_args(&sg, args + sp);
-    __syncthreads();
-    gram_fixed_body<T, CONJ, L, NB>(sg, sbid, pd[sp].nblk, smraw);
-    __syncthreads();
-  }
+  for_items(l, kClsBlas, args, &sg,
+            [&](int p, int64_t bid) { gram_fixed_body<T, CONJ, L, NB>(sg, bid, pd[p].nblk, smraw); });
 }
 
 // out = sum of the problem's partials, into its sp.g2 (grid: width tiles x nprob)
@@ -201,45 +207,14 @@ __global__ void __launch_bounds__(256) batch_update_kernel(const UpdateArgs* arg
   if (skip_first && l.ctl[1] == 0) return;   // first iteration: P = R already
   extern __shared__ __align__(16) unsigned char smraw[];
   __shared__ __align__(16) UpdateArgs su;
-  __shared__ int sp;
-  __shared__ int64_t sbid;
-  const int64_t total = l.total[kClsBlas];
-  for (int64_t item = blockIdx.x; item < total; item += gridDim.x) {
-    if (threadIdx.x == 0) {
-      int p;
-      int64_t bid;
-      list_find(l, kClsBlas, item, &p, &bid);
-      sp = p;
-      sbid = bid;
-    }
-    __syncthreads();
-    load_args(&su, args + sp);
-    __syncthreads();
-    update_fixed_body<T, A, L>(su, sbid, pd[sp].nblk, smraw);
-    __syncthreads();
-  }
+  for_items(l, kClsBlas, args, &su,
+            [&](int p, int64_t bid) { update_fixed_body<T, A, L>(su, bid, pd[p].nblk, smraw); });
 }
 
 template <typename T>
 __global__ void __launch_bounds__(256) batch_dots_kernel(const DotArgs* args, const ProbDev* pd, ListDev l) {
   __shared__ __align__(16) DotArgs sd;
-  __shared__ int sp;
-  __shared__ int64_t sbid;
-  const int64_t total = l.total[kClsBlas];
-  for (int64_t item = blockIdx.x; item < total; item += gridDim.x) {
-    if (threadIdx.x == 0) {
-      int p;
-      int64_t bid;
-      list_find(l, kClsBlas, item, &p, &bid);
-      sp = p;
-      sbid = bid;
-    }
-    __syncthreads();
-    load_args(&sd, args + sp);
-    __syncthreads();
-    dots_body<T>(sd, sbid, pd[sp].nblk);
-    __syncthreads();
-  }
+  for_items(l, kClsBlas, args, &sd, [&](int p, int64_t bid) { dots_body<T>(sd, bid, pd[p].nblk); });
 }
 
 // Elementwise steps over one problem's n values.
@@ -289,23 +264,7 @@ __device__ __forceinline__ void elem_body(const ElemArgs& e, int op, int64_t bid
 template <typename T>
 __global__ void __launch_bounds__(256) batch_elem_kernel(const ElemArgs* args, const ProbDev* pd, ListDev l, int op) {
   __shared__ __align__(16) ElemArgs se;
-  __shared__ int sp;
-  __shared__ int64_t sbid;
-  const int64_t total = l.total[kClsBlas];
-  for (int64_t item = blockIdx.x; item < total; item += gridDim.x) {
-    if (threadIdx.x == 0) {
-      int p;
-      int64_t bid;
-      list_find(l, kClsBlas, item, &p, &bid);
-      sp = p;
-      sbid = bid;
-    }
-    __syncthreads();
-    load_args(&se, args + sp);
-    __syncthreads();
-    elem_body<T>(se, op, sbid, pd[sp].nblk);
-    __syncthreads();
-  }
+  for_items(l, kClsBlas, args, &se, [&](int p, int64_t bid) { elem_body<T>(se, op, bid, pd[p].nblk); });
 }
 
 // ---- one CTA per problem ------------------------------------------------------------
