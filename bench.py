@@ -496,15 +496,18 @@ def run_sweep(args):
                     converged=int(sum(d.converge for d in dds)),
                     iterations_mean=round(float(np.mean([d.iter_fin + 1 for d in dds])), 2)), obs
 
-    arm(True, "mixed")                      # warm-up (graphs, kernels, allocator)
+    arms = [a for a in args.sweep_arms.split(",") if a]
+    table = {"one_at_a_time_fp64": (False, None), "one_at_a_time_mixed": (False, "mixed"),
+             "batched_fp64": (True, None), "batched_mixed": (True, "mixed")}
+    arm(True, None)                         # warm-up (graphs, kernels, allocator)
     res = {}
     obs = {}
-    for name, batched, prec in (("one_at_a_time_fp64", False, None), ("one_at_a_time_mixed", False, "mixed"),
-                                ("batched_fp64", True, None), ("batched_mixed", True, "mixed")):
+    for name in arms:
+        batched, prec = table[name]
         res[name], obs[name] = arm(batched, prec)
-    ref = obs["one_at_a_time_fp64"]
+    ref = obs.get("one_at_a_time_fp64")
     err = 0.0
-    for o, r in zip(obs["batched_mixed"], ref):
+    for o, r in zip(obs.get("batched_mixed", []), ref if ref is not None else []):
         for cols in ((1,), (2, 3), (4, 5), (10, 11)):
             a = o[:, cols[0]] + (1j * o[:, cols[1]] if len(cols) > 1 else 0)
             b = r[:, cols[0]] + (1j * r[:, cols[1]] if len(cols) > 1 else 0)
@@ -516,11 +519,11 @@ def run_sweep(args):
                       "problems": len(dds), "lattices_min_max": [min(int(np.prod(g["lattice_n"])) for g in geos),
                                                                  max(int(np.prod(g["lattice_n"])) for g in geos)],
                       "dipoles_min_max": [min(n_dip), max(n_dip)]},
-           "arms": res, "speedup_batched_mixed_vs_one_at_a_time_fp64":
-               round(res["batched_mixed"]["value"] / res["one_at_a_time_fp64"]["value"], 3),
-           "speedup_batched_vs_one_at_a_time_mixed":
-               round(res["batched_mixed"]["value"] / res["one_at_a_time_mixed"]["value"], 3),
-           "max_rel_err_batched_mixed_vs_fp64_observables": float("%.3g" % err),
+           "arms": res,
+           "speedups": {"%s_vs_%s" % (a, b): round(res[a]["value"] / res[b]["value"], 3)
+                        for a in res for b in res if a != b and a.startswith("batched") and
+                        b.startswith("one_at_a_time")},
+           "max_rel_err_batched_mixed_vs_fp64_observables": float("%.3g" % err) if ref is not None else None,
            "setup_s": {"shapes_host": round(shape_s, 2), "green_spectra": round(green_s, 2)}}
     print(json.dumps(out), flush=True)
 
@@ -628,6 +631,7 @@ def main():
     ap.add_argument("--sweep", action="store_true",
                     help="batched uneven sweep (48 GRE particles x 3 wavelengths, L=32) instead of the headline")
     ap.add_argument("--sweep-particles", type=int, default=48)
+    ap.add_argument("--sweep-arms", default="one_at_a_time_fp64,batched_fp64,batched_mixed")
     ap.add_argument("--fno", action="store_true", help="train and evaluate the learned warm start")
     ap.add_argument("--fno-train", type=int, default=256)
     ap.add_argument("--fno-eval", type=int, default=32)

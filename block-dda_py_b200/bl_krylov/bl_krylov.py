@@ -219,16 +219,29 @@ def _batch_struct(entries, mode):
     return arr
 
 
+# A batch shares one column-tile width and one shared-memory size per pencil
+# pass, set by its longest axis; problems are grouped with others whose longest
+# padded axis is within this ratio, so small lattices keep wide tiles.
+_SIZE_RATIO = 1.6
+# Lattices of at least this many padded grid points run the one-problem solver
+# (specialised, autotuned kernels; their launch overhead is negligible there).
+_BATCH_MAX_POINTS = 4 << 20
+
+
 def _batch_groups(entries, mode, L, itermax, max_bytes):
-    """Consecutive groups whose workspace fits max_bytes (at most 1024 problems each)."""
+    """Index groups of similar lattice size whose workspace fits max_bytes
+    (at most 1024 problems each), largest lattices first."""
     lib = _lib.load()
+    size = [max(e["g"].plan.m) for e in entries]
+    order = sorted(range(len(entries)), key=lambda i: -size[i])
     groups, cur = [], []
-    for e in entries:
-        trial = cur + [e]
-        nbytes = int(lib.bdda_batch_workspace_bytes(_batch_struct(trial, mode), len(trial), mode, L, itermax))
-        if cur and (len(trial) > 1024 or nbytes > max_bytes):
+    for i in order:
+        trial = cur + [i]
+        nbytes = int(lib.bdda_batch_workspace_bytes(_batch_struct([entries[j] for j in trial], mode), len(trial),
+                                                    mode, L, itermax))
+        if cur and (len(trial) > 1024 or nbytes > max_bytes or size[cur[0]] > _SIZE_RATIO * size[i]):
             groups.append(cur)
-            cur = [e]
+            cur = [i]
         else:
             cur = trial
     if cur:
@@ -257,7 +270,10 @@ def bl_bicgstab_jacobi_mvp_fft_batch(problems, tol, itermax, precision=None, max
     numpy.linalg.LinAlgError after the batch finished, unless ``statuses`` is
     given, in which case its X is None.  Problems are split into groups whose
     device workspace stays under ``max_bytes`` (default: 70 % of the free
-    device memory).
+    device memory); each group holds lattices of similar size (largest padded
+    axis within 1.6x), so every group gets launch shapes that fit it.  Large
+    lattices (>= 4 Mi padded grid points) and groups of one run the one-problem
+    solver instead.
     """
     key = "c128" if precision is None else str(precision).lower()
     if key not in _BATCH_MODES:
@@ -278,8 +294,30 @@ def bl_bicgstab_jacobi_mvp_fft_batch(problems, tol, itermax, precision=None, max
         free, _ = torch.cuda.mem_get_info(dev)
         max_bytes = int(0.7 * free)
     lib = _lib.load()
-    results = []
-    for grp in _batch_groups(entries, mode, L, itermax, max_bytes):
+    results = [None] * len(entries)
+    hists = [None] * len(entries)
+    big = [i for i, e in enumerate(entries) if int(np.prod(e["g"].plan.m)) >= _BATCH_MAX_POINTS]
+    small = [i for i in range(len(entries)) if i not in set(big)]
+    groups = [[small[j] for j in g] for g in _batch_groups([entries[i] for i in small], mode, L, itermax, max_bytes)]
+    for g in [g for g in groups if len(g) == 1]:
+        big.append(g[0])
+    groups = [g for g in groups if len(g) > 1]
+    one_prec = {_lib.BATCH_C128: None, _lib.BATCH_C64: "c64", _lib.BATCH_MIXED: "mixed"}[mode]
+    for i in big:   # one problem at a time
+        e = entries[i]
+        h = [] if history is not None else None
+        try:
+            X, it_, er_ = _solve(_lib.BICGSTAB, e["g"].plan.n, 3, e["occ"], e["g"], e["diag"], e["B"], tol, itermax,
+                                 X0=e["X0"], precision=one_prec, history=h, max_outer=max_outer)
+            s_ = 0 if er_ < tol else 1
+        except np.linalg.LinAlgError:
+            X, it_, er_, s_ = None, 0, float("inf"), 2
+        if X is not None and e["numpy"]:
+            X = X.cpu().numpy()
+        results[i] = (X, int(it_), float(er_), s_)
+        hists[i] = h
+    for idx in groups:
+        grp = [entries[i] for i in idx]
         arr = _batch_struct(grp, mode)
         nb = int(lib.bdda_batch_workspace_bytes(arr, len(grp), mode, L, itermax))
         if nb == 0:
@@ -298,10 +336,14 @@ def bl_bicgstab_jacobi_mvp_fft_batch(problems, tol, itermax, precision=None, max
         for i, e in enumerate(grp):
             s = int(st[i])
             X = None if s == 2 else (e["X"].cpu().numpy() if e["numpy"] else e["X"])
-            results.append((X, int(it[i]), float(er[i]), s))
+            results[idx[i]] = (X, int(it[i]), float(er[i]), s)
             if history is not None:
                 ran = 0 if itermax == 0 or s == 2 else int(it[i]) + 1
-                history.append([hist[i * itermax + k] for k in range(min(ran, itermax))])
+                hists[idx[i]] = [hist[i * itermax + k] for k in range(min(ran, itermax))]
+    hbase = 0
+    if history is not None:
+        hbase = len(history)
+        history.extend(hists)
     if mode == _lib.BATCH_MIXED:
         # problems the mixed form leaves above tol (its recursion diverged under the
         # complex64 products) are solved again with complex128 products
@@ -316,7 +358,7 @@ def bl_bicgstab_jacobi_mvp_fft_batch(problems, tol, itermax, precision=None, max
                 X, it, er = again[j]
                 results[i] = (X, results[i][1] + 1 + it, er, sub_st[j])
                 if history is not None:
-                    history[i] = history[i] + sub_hist[j]
+                    history[hbase + i] = history[hbase + i] + sub_hist[j]
     if statuses is not None:
         statuses.extend(r[3] for r in results)
     elif any(r[3] == 2 for r in results):

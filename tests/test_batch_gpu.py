@@ -158,5 +158,5 @@ def test_groups_split_by_workspace(bk, batch):
     ents = [bk._batch_entry(a) for a in args]
     one = int(_lib.load().bdda_batch_workspace_bytes(bk._batch_struct(ents[1:2], 0), 1, 0, 8, 200))
     split = bk.bl_bicgstab_jacobi_mvp_fft_batch(args, 1e-6, 200, max_bytes=one + 1)
-    for (Xa, ia, ea), (Xb, ib, eb) in zip(full, split):
-        assert abs(ia - ib) <= 1 and rel(Xa, Xb) < 1e-4
+    for (Xa, ia, ea), (Xb, ib, eb) in zip(full, split):   # groups of one run the one-problem solver
+        assert ea < 1e-6 and eb < 1e-6 and abs(ia - ib) <= 3 and rel(Xa, Xb) < 1e-4
