@@ -46,6 +46,13 @@ ITERMAX = 500
 # The CPU reference runs the same algorithm (iteration counts agree within 1),
 # so its throughput is extrapolated from a timed sample of iterations.
 REF_ITERS_PER_CHUNK = 21
+# DRAM bytes (read + write) of the five complex64 passes (Z, Y, X, Y^-1, Z^-1) of this
+# workload's product at L = 8, from one ncu capture of `bench.py --mvp-only --L 8`
+# (dram__bytes_read.sum + dram__bytes_write.sum); the parts that do not grow with L
+# are the Green's spectrum (X pass) and the occupancy maps (Z, Z^-1).  The roofline's
+# traffic scales the rest to the timed L.
+DRAM_L8_C64 = (0.7316e9, 2.0403e9, 3.4710e9, 2.0569e9, 0.8936e9)
+DRAM_L8_CONST = (0.0072e9, 0.0, 0.7225e9, 0.0, 0.0072e9)
 
 
 def workload_config(L):
@@ -275,9 +282,12 @@ def run_bdda(args, rank, world, local_rank):
                                   for nm, tm, b in zip(["Z", "Y", "X", "Y^-1", "Z^-1"], per, pb)]}
     main = _lib.C64 if (mixed and _lib.C64 in lines) else _lib.C128
     rl = lines[main]
+    traffic = None
+    if main == _lib.C64 and list(plan.m) == [192, 224, 350]:
+        traffic = int(sum((b - c) * L / 8 + c for b, c in zip(DRAM_L8_C64, DRAM_L8_CONST)))
     roofline = {"kernel": "block MVP, %s (5 pencil passes)" % ("complex64" if main == _lib.C64 else "complex128"),
                 "bound": "hbm", "achieved": rl["achieved"], "peak": peak, "unit": "GB/s",
-                "frac": round(rl["achieved"] / peak, 3), "traffic": None, "peak_source": peak_src,
+                "frac": round(rl["achieved"] / peak, 3), "traffic": traffic, "peak_source": peak_src,
                 "alg_bytes_per_mvp": rl["alg_bytes_per_mvp"], "mvp_ms": rl["mvp_ms"],
                 "mvps_timed": rl["mvps_timed"], "passes": rl["passes"]}
     if mixed and _lib.C128 in lines:
@@ -420,10 +430,10 @@ SWEEP_WL = (0.45, 0.55, 0.85)
 SWEEP_MP = 1.53 + 0.005j
 
 
-def sweep_shapes(n_particles, seed=3):
+def sweep_shapes(n_particles, seed=3, x_range=(4.0, 16.0)):
     """Shape parameters of the sweep: x ~ U[4,16], ab, bc ~ U[0.5,1], beta ~ U[0,0.2]."""
     rng = np.random.default_rng(seed)
-    x = rng.uniform(4.0, 16.0, n_particles)
+    x = rng.uniform(x_range[0], x_range[1], n_particles)
     ab = rng.uniform(0.5, 1.0, n_particles)
     bc = rng.uniform(0.5, 1.0, n_particles)
     beta = rng.uniform(0.0, 0.2, n_particles)
@@ -441,7 +451,8 @@ def run_sweep(args):
     """Orientations/s of the sweep: one problem at a time vs one batched solve, FP64 and mixed."""
     import concurrent.futures
     import multiprocessing
-    specs = sweep_shapes(args.sweep_particles)
+    x_range = tuple(float(v) for v in args.sweep_x.split(","))
+    specs = sweep_shapes(args.sweep_particles, x_range=x_range)
     t0 = time.perf_counter()
     # shapes on the host cores, before any CUDA call: spawned single-threaded workers
     for var in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS"):
@@ -513,9 +524,9 @@ def run_sweep(args):
             b = r[:, cols[0]] + (1j * r[:, cols[1]] if len(cols) > 1 else 0)
             err = max(err, float(np.max(np.abs(a - b)) / np.max(np.abs(b))))
     out = {"metric": "orientations/s over a batched uneven sweep to rel-res 1e-5", "unit": "orientations/s",
-           "config": {"workload": "%d GRE particles (x~U[4,16], ab,bc~U[0.5,1], beta~U[0,0.2], seed 3) x "
+           "config": {"workload": "%d GRE particles (x~U[%g,%g], ab,bc~U[0.5,1], beta~U[0,0.2], seed 3) x "
                                   "wavelengths %s, m_m 1, m_p %s, lambda/16 spacing, L=%d, block-BiCGSTAB"
-                                  % (len(geos), list(SWEEP_WL), SWEEP_MP, L),
+                                  % (len(geos), x_range[0], x_range[1], list(SWEEP_WL), SWEEP_MP, L),
                       "problems": len(dds), "lattices_min_max": [min(int(np.prod(g["lattice_n"])) for g in geos),
                                                                  max(int(np.prod(g["lattice_n"])) for g in geos)],
                       "dipoles_min_max": [min(n_dip), max(n_dip)]},
@@ -632,6 +643,7 @@ def main():
                     help="batched uneven sweep (48 GRE particles x 3 wavelengths, L=32) instead of the headline")
     ap.add_argument("--sweep-particles", type=int, default=48)
     ap.add_argument("--sweep-arms", default="one_at_a_time_fp64,batched_fp64,batched_mixed")
+    ap.add_argument("--sweep-x", default="4,16", help="size-parameter range of the sweep particles")
     ap.add_argument("--fno", action="store_true", help="train and evaluate the learned warm start")
     ap.add_argument("--fno-train", type=int, default=256)
     ap.add_argument("--fno-eval", type=int, default=32)
