@@ -180,6 +180,11 @@ def run_bdda(args, rank, world, local_rank):
     torch.cuda.synchronize()
     green_s = time.perf_counter() - t0
     green = dd.Au_til
+    # launch shapes of this lattice's pencil passes, like FFT planning (untimed)
+    from bdda_b200.runtime import autotune
+    t0 = time.perf_counter()
+    tuned = {p: autotune(green, dd._dev["occ"], L, p, reps=2) for p in ("c128", "c64")}
+    tune_s = time.perf_counter() - t0
 
     def device_step(d):
         d.set_interaction_matrix(green=green)
@@ -304,7 +309,8 @@ def run_bdda(args, rank, world, local_rank):
         "form": args.form,
         "data": "synthetic: reference GRE geometry (seed 1) and SO(3) orientations (seed 2)",
         "config": dict(workload_config(L), parallelism="replicas x%d" % world,
-                       green_build_s=round(green_s, 4), iterations=iters, converged=dd.converge,
+                       green_build_s=round(green_s, 4), autotune_s=round(tune_s, 2),
+                       autotune_mvp_ms={k: [round(v[0], 3), round(v[1], 3)] for k, v in tuned.items()}, iterations=iters, converged=dd.converge,
                        true_residual=dd.err_fin if mixed else None),
         "plain_fp64": plain,
         "e2e": {"value": round(world * L / e2e_s, 3), "unit": "orientations/s",

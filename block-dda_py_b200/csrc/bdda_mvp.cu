@@ -105,9 +105,9 @@ static FixedLaunchFn fixed_find(int prec, int kind, int lt, const AxisFFT& ax, i
   int r[4] = {1, 1, 1, 1};
   for (int s = 0; s < ax.nst; ++s) r[s] = ax.rad[s];
   FixedLaunchFn first = nullptr;
-  for (int t = 0; t < 2; ++t) {
+  for (int t = 0; t < 3; ++t) {
     int n = 0;
-    const FixedKernel* tab = t == 0 ? fixed_table_a(&n) : fixed_table_b(&n);
+    const FixedKernel* tab = t == 0 ? fixed_table_a(&n) : t == 1 ? fixed_table_b(&n) : fixed_table_c(&n);
     for (int i = 0; i < n; ++i) {
       const FixedKernel& f = tab[i];
       if (f.prec == prec && f.kind == kind && f.lt == lt && f.r[0] == r[0] && f.r[1] == r[1] &&
@@ -126,9 +126,9 @@ static std::vector<int> fixed_variants(int prec, int kind, int lt, const AxisFFT
   if (ax.nst > 4) return out;
   int r[4] = {1, 1, 1, 1};
   for (int s = 0; s < ax.nst; ++s) r[s] = ax.rad[s];
-  for (int t = 0; t < 2; ++t) {
+  for (int t = 0; t < 3; ++t) {
     int n = 0;
-    const FixedKernel* tab = t == 0 ? fixed_table_a(&n) : fixed_table_b(&n);
+    const FixedKernel* tab = t == 0 ? fixed_table_a(&n) : t == 1 ? fixed_table_b(&n) : fixed_table_c(&n);
     for (int i = 0; i < n; ++i) {
       const FixedKernel& f = tab[i];
       if (f.prec == prec && f.kind == kind && f.lt == lt && f.r[0] == r[0] && f.r[1] == r[1] &&

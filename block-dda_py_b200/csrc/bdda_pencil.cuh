@@ -430,6 +430,7 @@ struct FixedKernel {
 };
 const FixedKernel* fixed_table_a(int* n);
 const FixedKernel* fixed_table_b(int* n);
+const FixedKernel* fixed_table_c(int* n);
 
 
 }  // namespace bdda
