@@ -53,9 +53,9 @@ __device__ __forceinline__ void fixed_mid(const PassArgs& a, const Pen& c, T* sm
   }
 }
 
-// MINB: resident CTAs per SM the register allocation must allow (the
-// __launch_bounds__ minimum); 1 = no bound.  complex128 kernels are compiled
-// with 3 and 4 and the autotuner picks per pass.
+// NT: threads per CTA.  MINB: resident CTAs per SM the register allocation
+// must allow (the __launch_bounds__ minimum); 1 = no bound.  Kernels are
+// compiled with several (NT, MINB) and the autotuner picks per pass.
 template <typename T, int KIND, int LT, int NT, int MINB, int R0, int R1, int R2, int R3>
 __global__ void __launch_bounds__(NT, MINB) fixed_pencil_kernel(const PassArgs a) {
   using RS = RadixSeq<R0, R1, R2, R3>;
@@ -104,9 +104,8 @@ __global__ void __launch_bounds__(NT, MINB) fixed_pencil_kernel(const PassArgs a
   }
 }
 
-template <typename T, int KIND, int LT, int MINB, int R0, int R1, int R2, int R3>
+template <typename T, int KIND, int LT, int MINB, int NT, int R0, int R1, int R2, int R3>
 int fixed_launch(const PassArgs& a0, int64_t P0, cudaStream_t st) {
-  constexpr int NT = 256;
   using RS = RadixSeq<R0, R1, R2, R3>;
   PassArgs a = a0;
   if (a.ax.M != RS::M) return BDDA_BAD_ARG;
@@ -124,7 +123,13 @@ int fixed_launch(const PassArgs& a0, int64_t P0, cudaStream_t st) {
   return BDDA_OK;
 }
 
+// Table entry of a specialised kernel with 256 threads per CTA (variant id =
+// MINB) or NT threads (variant id = MINB + 16 NT/32: the CTA size that makes
+// the stages' butterfly jobs fill whole rounds of threads).
 #define BDDA_FIXED(T, PREC, KIND, LT, MINB, R0, R1, R2, R3) \
-  { PREC, KIND, LT, MINB, {R0, R1, R2, R3}, &fixed_launch<T, KIND, LT, MINB, R0, R1, R2, R3> }
+  { PREC, KIND, LT, MINB, MINB, {R0, R1, R2, R3}, &fixed_launch<T, KIND, LT, MINB, 256, R0, R1, R2, R3> }
+#define BDDA_FIXED_NT(T, PREC, KIND, LT, MINB, NT, R0, R1, R2, R3)                              \
+  { PREC, KIND, LT, MINB, MINB + 16 * ((NT) / 32), {R0, R1, R2, R3},                              \
+    &fixed_launch<T, KIND, LT, MINB, NT, R0, R1, R2, R3> }
 
 }  // namespace bdda

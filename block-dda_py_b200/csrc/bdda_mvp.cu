@@ -98,6 +98,16 @@ static int launch_lt(PassArgs a, int64_t P0, cudaStream_t st) {
 
 static int g_use_fixed = 1;   // specialised kernels on (bdda_tune_fixed)
 
+static const FixedKernel* fixed_table(int t, int* n) {
+  switch (t) {
+    case 0: return fixed_table_a(n);
+    case 1: return fixed_table_b(n);
+    case 2: return fixed_table_c(n);
+    case 3: return fixed_table_d(n);
+    default: return fixed_table_e(n);
+  }
+}
+
 // Specialised kernel for (precision, kind, tile width, radix sequence);
 // variant as in PassTune.
 static FixedLaunchFn fixed_find(int prec, int kind, int lt, const AxisFFT& ax, int variant) {
@@ -105,14 +115,14 @@ static FixedLaunchFn fixed_find(int prec, int kind, int lt, const AxisFFT& ax, i
   int r[4] = {1, 1, 1, 1};
   for (int s = 0; s < ax.nst; ++s) r[s] = ax.rad[s];
   FixedLaunchFn first = nullptr;
-  for (int t = 0; t < 3; ++t) {
+  for (int t = 0; t < 5; ++t) {
     int n = 0;
-    const FixedKernel* tab = t == 0 ? fixed_table_a(&n) : t == 1 ? fixed_table_b(&n) : fixed_table_c(&n);
+    const FixedKernel* tab = fixed_table(t, &n);
     for (int i = 0; i < n; ++i) {
       const FixedKernel& f = tab[i];
       if (f.prec == prec && f.kind == kind && f.lt == lt && f.r[0] == r[0] && f.r[1] == r[1] &&
           f.r[2] == r[2] && f.r[3] == r[3]) {
-        if (variant == 0 || f.minb == variant) return f.fn;
+        if (variant == 0 || f.variant == variant) return f.fn;
         if (!first) first = f.fn;
       }
     }
@@ -126,14 +136,14 @@ static std::vector<int> fixed_variants(int prec, int kind, int lt, const AxisFFT
   if (ax.nst > 4) return out;
   int r[4] = {1, 1, 1, 1};
   for (int s = 0; s < ax.nst; ++s) r[s] = ax.rad[s];
-  for (int t = 0; t < 3; ++t) {
+  for (int t = 0; t < 5; ++t) {
     int n = 0;
-    const FixedKernel* tab = t == 0 ? fixed_table_a(&n) : t == 1 ? fixed_table_b(&n) : fixed_table_c(&n);
+    const FixedKernel* tab = fixed_table(t, &n);
     for (int i = 0; i < n; ++i) {
       const FixedKernel& f = tab[i];
       if (f.prec == prec && f.kind == kind && f.lt == lt && f.r[0] == r[0] && f.r[1] == r[1] &&
           f.r[2] == r[2] && f.r[3] == r[3])
-        out.push_back(f.minb);
+        out.push_back(f.variant);
     }
   }
   return out;
@@ -519,7 +529,7 @@ int bdda_tune_set(int prec, int kind, size_t smem_budget, int threads) {
 
 int bdda_tune_pass(int prec, int kind, int M, int L, int lt, int variant) {
   if (prec < 0 || prec > 1 || kind < 0 || kind > 2 || M < 1 || L < 1 || L > kMaxL ||
-      (lt != 0 && lt != 2 && lt != 4 && lt != 8) || variant < -1 || variant > 8)
+      (lt != 0 && lt != 2 && lt != 4 && lt != 8) || variant < -1 || variant > 1024)
     return BDDA_BAD_ARG;
   set_pass_tune({prec, kind, M, L, lt, variant});
   return BDDA_OK;

@@ -425,12 +425,15 @@ typedef int (*FixedLaunchFn)(const PassArgs& a, int64_t P0, cudaStream_t st);
 struct FixedKernel {
   int prec, kind, lt;
   int minb;            // register bound: resident CTAs per SM (1 = none)
+  int variant;         // id for the autotuner: minb (256 threads) or minb + 16 * threads / 32
   int r[4];            // radix sequence, padded with 1
   FixedLaunchFn fn;
 };
 const FixedKernel* fixed_table_a(int* n);
 const FixedKernel* fixed_table_b(int* n);
 const FixedKernel* fixed_table_c(int* n);
+const FixedKernel* fixed_table_d(int* n);
+const FixedKernel* fixed_table_e(int* n);
 
 
 }  // namespace bdda

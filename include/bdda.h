@@ -90,7 +90,8 @@ int bdda_tune_get(int prec, int kind, size_t* smem_budget, int* threads);
 /* Per-pass launch choice for passes of (prec, kind) over an axis of length M
  * at block width L: column tile width lt (2, 4, 8; 0 = the smem_budget rule)
  * and kernel variant (0 = the first specialised kernel compiled for the radix
- * sequence, k > 0 = the one compiled for k resident CTAs per SM, -1 = the
+ * sequence; k in 1..8 = the one of 256 threads compiled for k resident CTAs
+ * per SM; k + 16 * (threads / 32) = the one of that CTA size; -1 = the
  * generic run-time-radix kernel).  Process-wide; set by bdda_autotune. */
 int bdda_tune_pass(int prec, int kind, int M, int L, int lt, int variant);
 int bdda_tune_pass_get(int prec, int kind, int M, int L, int* lt, int* variant);
