@@ -51,6 +51,9 @@ __device__ __forceinline__ void gram_reduce_body(const double2* partial, int nbl
 }
 
 // ---- Gram, specialised on L: split-K over row chunks, register tiles --------
+// A thread owns rows ty + NT i and columns tx + NT j of the L x L tile, so the
+// 32 lanes of a warp read consecutive 16-byte words of a staged row (no
+// shared-memory bank conflicts).
 // Each CTA reduces a contiguous range of rows into a full L x L partial (per
 // B matrix); row chunks of RCH rows are double-buffered in shared memory with
 // cp.async so the next chunk streams in while the current one is consumed.
@@ -118,13 +121,13 @@ __device__ __forceinline__ void gram_fixed_body(const GramArgs& g, int64_t bid, 
         double2 a[TM], b[NB][TM];
 #pragma unroll
         for (int ii = 0; ii < TM; ++ii) {
-          a[ii] = to_d2(sA[r * L + ty * TM + ii]);
+          a[ii] = to_d2(sA[r * L + ty + NT * ii]);
           if (CONJ) a[ii].y = -a[ii].y;
         }
 #pragma unroll
         for (int k = 0; k < NB; ++k)
 #pragma unroll
-          for (int jj = 0; jj < TM; ++jj) b[k][jj] = to_d2(sA[(1 + k) * CH + r * L + tx * TM + jj]);
+          for (int jj = 0; jj < TM; ++jj) b[k][jj] = to_d2(sA[(1 + k) * CH + r * L + tx + NT * jj]);
 #pragma unroll
         for (int k = 0; k < NB; ++k)
 #pragma unroll
@@ -143,14 +146,15 @@ __device__ __forceinline__ void gram_fixed_body(const GramArgs& g, int64_t bid, 
       for (int ii = 0; ii < TM; ++ii)
 #pragma unroll
         for (int jj = 0; jj < TM; ++jj)
-          g.partial[((bid * NB + k) * L + ty * TM + ii) * L + tx * TM + jj] = acc[k][ii][jj];
+          g.partial[((bid * NB + k) * L + ty + NT * ii) * L + tx + NT * jj] = acc[k][ii][jj];
   }
 }
 
 // ---- block update, specialised on L ---------------------------------------------
 // out = a0 Y0 + a1 Y1 + (X1 + c2 X2) M.  M lives in shared memory for the
 // whole kernel; X row blocks of RB rows are staged per iteration; each thread
-// owns TR rows x TC columns of the output block.
+// owns TR rows x TC columns (cg + NCG j) of the output block, so lanes read
+// consecutive 16-byte words of M (no shared-memory bank conflicts).
 template <typename T, typename A, int L>
 __device__ __forceinline__ void update_fixed_body(const UpdateArgs& u, int64_t bid, int64_t nblk, unsigned char* ufs) {
   constexpr int TC = L >= 64 ? 4 : (L >= 32 ? 2 : 1);
@@ -196,7 +200,7 @@ __device__ __forceinline__ void update_fixed_body(const UpdateArgs& u, int64_t b
       for (int jj = 0; jj < TC; ++jj) {
         acc[ii][jj] = conv_acc<A>(make_double2(0.0, 0.0));
         if (row < u.n) {
-          const int64_t idx = row * L + cg * TC + jj;
+          const int64_t idx = row * L + cg + NCG * jj;
           if (Y0) acc[ii][jj] = cfma(a0, ld_as<A>(Y0, idx), acc[ii][jj]);
           if (Y1) acc[ii][jj] = cfma(a1, ld_as<A>(Y1, idx), acc[ii][jj]);
         }
@@ -209,7 +213,7 @@ __device__ __forceinline__ void update_fixed_body(const UpdateArgs& u, int64_t b
 #pragma unroll
         for (int ii = 0; ii < TR; ++ii) x[ii] = sX[(rg * TR + ii) * L + i];
 #pragma unroll
-        for (int jj = 0; jj < TC; ++jj) m[jj] = sM[i * L + cg * TC + jj];
+        for (int jj = 0; jj < TC; ++jj) m[jj] = sM[i * L + cg + NCG * jj];
 #pragma unroll
         for (int ii = 0; ii < TR; ++ii)
 #pragma unroll
@@ -223,7 +227,7 @@ __device__ __forceinline__ void update_fixed_body(const UpdateArgs& u, int64_t b
 #pragma unroll
         for (int jj = 0; jj < TC; ++jj) {
           const T v = st_as<T>(acc[ii][jj]);
-          out[row * L + cg * TC + jj] = v;
+          out[row * L + cg + NCG * jj] = v;
           const double2 vd = to_d2(v);
           nrm += vd.x * vd.x + vd.y * vd.y;
         }
