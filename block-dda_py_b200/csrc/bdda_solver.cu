@@ -898,6 +898,11 @@ static int run_mixed(int solver, const bdda_plan* p, int L, int n_occ, const voi
         *iter_fin = total - 1;
       }
       max_outer = round + 1;   // this is the last round
+    } else if (solver == BDDA_BICGSTAB && s_in == BDDA_OK) {
+      // BiCGSTAB stopped on a replaced residual: it is the true residual already
+      *err_fin = err_in;
+      status = BDDA_OK;
+      break;
     }
     // true residual with the complex128 product
     c.ghat32 = nullptr;
