@@ -4,8 +4,10 @@
 // every butterfly job pays integer divisions and strides it cannot fold.
 // Here the sequence (up to four radices, padded with 1), the tile width and
 // the CTA size are template parameters: stage spans, twiddle strides, job
-// counts and all index divisions are constants, and each stage's job loop
-// unrolls.  bdda_fixed_*.cu instantiate the sequences the planner produces
+// counts and all index divisions are constants.  Each butterfly unrolls; the
+// loop over a stage's rounds of jobs does not (unrolling it made the kernels
+// large enough to stall on instruction fetch: the complex64 product ran 3 %
+// slower).  bdda_fixed_*.cu instantiate the sequences the planner produces
 // for the workloads; fixed_find() in bdda_mvp.cu dispatches to them.
 #pragma once
 #include "bdda_pencil.cuh"
@@ -28,7 +30,7 @@ __device__ __forceinline__ void fixed_stage(const PassArgs& a, const Pen& c, T* 
   constexpr int R = RS::r(S), B = RS::blk(S), SPAN = B / R, TSTEP = RS::M / B;
   constexpr int NJOBS = (RS::M / R) * W;
   constexpr int ITERS = (NJOBS + NT - 1) / NT;
-#pragma unroll
+#pragma unroll 1
   for (int it = 0; it < ITERS; ++it) {
     const int job = threadIdx.x + it * NT;
     if ((NJOBS % NT) == 0 || job < NJOBS) {
@@ -46,7 +48,7 @@ __device__ __forceinline__ void fixed_mid(const PassArgs& a, const Pen& c, T* sm
   constexpr int R = RS::r(RS::n - 1);
   constexpr int NJOBS = (RS::M / R) * LT;
   constexpr int ITERS = (NJOBS + NT - 1) / NT;
-#pragma unroll
+#pragma unroll 1
   for (int it = 0; it < ITERS; ++it) {
     const int job = threadIdx.x + it * NT;
     if ((NJOBS % NT) == 0 || job < NJOBS) conv_mid_job<R, SRC, DST, T, LT>(a, c, sm, gs, job / LT, job % LT);
