@@ -404,6 +404,16 @@ def run_mvp_only(args):
     jpre = 1.0 / diag
     work = green.workspace(prec, args.L)
     gh = green.ghat(prec)
+    tune = None
+    if args.autotune:
+        from bdda_b200.runtime import autotune
+        autotune(green, occ, args.L, "c128" if prec == _lib.C128 else "c64", reps=2)
+        tune = []
+        for kind, ax in ((0, 2), (0, 1), (1, 0), (2, 1), (2, 2)):
+            lt, var = _lib.C.c_int(), _lib.C.c_int()
+            _lib.check(lib.bdda_tune_pass_get(prec, kind, int(plan.m[ax]), args.L, _lib.C.byref(lt),
+                                              _lib.C.byref(var)), "tune_pass_get")
+            tune.append([lt.value, var.value])
 
     def mvp():
         _lib.check(lib.bdda_block_mvp(plan.handle, prec, args.L, ptr(gh), ptr(occ.cell_map), ptr(diag),
@@ -426,7 +436,8 @@ def run_mvp_only(args):
                       "radices": [plan.radices(a) for a in range(3)], "mvp_ms": round(sum(per), 3),
                       "GB/s": round(sum(pb) / (sum(per) * 1e-3) / 1e9, 1),
                       "passes_ms": [round(x, 3) for x in per],
-                      "passes_GBs": [round(b / (t * 1e-3) / 1e9, 1) for b, t in zip(pb, per)]}), flush=True)
+                      "passes_GBs": [round(b / (t * 1e-3) / 1e9, 1) for b, t in zip(pb, per)],
+                      "tuned_lt_variant": tune}), flush=True)
 
 
 # ---------------------------------------------------------------------------
@@ -645,6 +656,7 @@ def main():
     ap.add_argument("--L", type=int, default=64)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--mvp-only", action="store_true", help="time block MVPs of the workload only")
+    ap.add_argument("--autotune", action="store_true", help="with --mvp-only: autotune the passes first")
     ap.add_argument("--sweep", action="store_true",
                     help="batched uneven sweep (48 GRE particles x 3 wavelengths, L=32) instead of the headline")
     ap.add_argument("--sweep-particles", type=int, default=48)

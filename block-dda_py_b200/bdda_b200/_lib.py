@@ -55,6 +55,7 @@ PROTOTYPES = {
                               _vp, _sz, _vp]),
     "bdda_batch_bicgstab": (_i, [_vp, _i, _i, _i, _d, _i, _i, _i, _pi, _pi, _pd, _pd, _vp, _sz, _vp]),
     "bdda_tune_pass_get": (_i, [_i, _i, _i, _i, _pi, _pi]),
+    "bdda_tune_pass_variants": (_i, [_vp, _i, _i, _i, _i, _pi, _i, _pi]),
     "bdda_autotune": (_i, [_vp, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i, _pd, _pd, _vp]),
     "bdda_plan_create": (_i, [_pi, _pi, C.POINTER(_vp)]),
     "bdda_plan_destroy": (None, [_vp]),

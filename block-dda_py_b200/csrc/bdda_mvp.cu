@@ -48,8 +48,9 @@ static_assert(K_FWD == 0 && K_CONV == 1 && K_INV == 2, "tuning tables are indexe
 // Per-pass launch choices set by the autotuner (bdda_tune_pass), keyed by
 // precision, pass kind, axis length and L: the column tile width lt (0 = the
 // shared-memory budget rule) and the kernel variant (0 = the first
-// specialised kernel compiled, k > 0 = the one compiled for k resident CTAs
-// per SM, -1 = the generic kernel).
+// specialised kernel compiled, k > 0 = the one with that id in the tables:
+// register bound, CTA size and column pairs as bdda_fixed.cuh numbers them,
+// -1 = the generic kernel).
 struct PassTune { int prec, kind, M, L, lt, variant; };
 static std::vector<PassTune> g_pass_tune;
 static std::mutex g_tune_mu;
@@ -98,30 +99,41 @@ static int launch_lt(PassArgs a, int64_t P0, cudaStream_t st) {
 
 static int g_use_fixed = 1;   // specialised kernels on (bdda_tune_fixed)
 
+static constexpr int kFixedTables = 7;
+
 static const FixedKernel* fixed_table(int t, int* n) {
   switch (t) {
     case 0: return fixed_table_a(n);
     case 1: return fixed_table_b(n);
     case 2: return fixed_table_c(n);
     case 3: return fixed_table_d(n);
-    default: return fixed_table_e(n);
+    case 4: return fixed_table_e(n);
+    case 5: return fixed_table_f(n);
+    default: return fixed_table_g(n);
   }
 }
 
+// Column-pair kernels read and write two complex64 values per access: L
+// even, every field pointer of the pass 16-byte aligned.
+static bool pair_ok(const PassArgs& a) {
+  auto al = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; };
+  return (a.L % 2) == 0 && al(a.src) && al(a.dst) && al(a.S);
+}
+
 // Specialised kernel for (precision, kind, tile width, radix sequence);
-// variant as in PassTune.
-static FixedLaunchFn fixed_find(int prec, int kind, int lt, const AxisFFT& ax, int variant) {
+// variant as in PassTune; column-pair kernels only if pairs (pair_ok).
+static FixedLaunchFn fixed_find(int prec, int kind, int lt, const AxisFFT& ax, int variant, bool pairs) {
   if (!g_use_fixed || variant < 0 || ax.nst > 4) return nullptr;
   int r[4] = {1, 1, 1, 1};
   for (int s = 0; s < ax.nst; ++s) r[s] = ax.rad[s];
   FixedLaunchFn first = nullptr;
-  for (int t = 0; t < 5; ++t) {
+  for (int t = 0; t < kFixedTables; ++t) {
     int n = 0;
     const FixedKernel* tab = fixed_table(t, &n);
     for (int i = 0; i < n; ++i) {
       const FixedKernel& f = tab[i];
       if (f.prec == prec && f.kind == kind && f.lt == lt && f.r[0] == r[0] && f.r[1] == r[1] &&
-          f.r[2] == r[2] && f.r[3] == r[3]) {
+          f.r[2] == r[2] && f.r[3] == r[3] && (pairs || !f.pair)) {
         if (variant == 0 || f.variant == variant) return f.fn;
         if (!first) first = f.fn;
       }
@@ -131,18 +143,18 @@ static FixedLaunchFn fixed_find(int prec, int kind, int lt, const AxisFFT& ax, i
 }
 
 // Register-bound variants compiled for (precision, kind, tile width, radix sequence).
-static std::vector<int> fixed_variants(int prec, int kind, int lt, const AxisFFT& ax) {
+static std::vector<int> fixed_variants(int prec, int kind, int lt, const AxisFFT& ax, bool pairs) {
   std::vector<int> out;
   if (ax.nst > 4) return out;
   int r[4] = {1, 1, 1, 1};
   for (int s = 0; s < ax.nst; ++s) r[s] = ax.rad[s];
-  for (int t = 0; t < 5; ++t) {
+  for (int t = 0; t < kFixedTables; ++t) {
     int n = 0;
     const FixedKernel* tab = fixed_table(t, &n);
     for (int i = 0; i < n; ++i) {
       const FixedKernel& f = tab[i];
       if (f.prec == prec && f.kind == kind && f.lt == lt && f.r[0] == r[0] && f.r[1] == r[1] &&
-          f.r[2] == r[2] && f.r[3] == r[3])
+          f.r[2] == r[2] && f.r[3] == r[3] && (pairs || !f.pair))
         out.push_back(f.variant);
     }
   }
@@ -153,7 +165,7 @@ template <typename T, int KIND>
 static int launch_pass(const PassArgs& a, int64_t P0, int lt, cudaStream_t st) {
   if (!a.green) {
     const int variant = pass_tune(prec_of<T>(), KIND, a.ax.M, a.L).variant;
-    FixedLaunchFn f = fixed_find(prec_of<T>(), KIND, lt, a.ax, variant);
+    FixedLaunchFn f = fixed_find(prec_of<T>(), KIND, lt, a.ax, variant, pair_ok(a));
     if (f) return f(a, P0, st);
   }
   switch (lt) {
@@ -291,6 +303,9 @@ static int autotune_impl(const bdda_plan* p, int L, const T* ghat, const int32_t
   };
   std::vector<Key> keys;
   int key_of[5];
+  PassArgs pa[5];
+  int64_t pp0[5];
+  mvp_pass_args<T>(p, L, ghat, cmap, S, diag, jpre, out, work, pa, pp0);
   for (int q = 0; q < 5; ++q) {
     const int M = p->ax[pass_axis[q]].M;
     int k = -1;
@@ -303,7 +318,8 @@ static int autotune_impl(const bdda_plan* p, int L, const T* ghat, const int32_t
       for (int lt : {8, 4, 2}) {
         if (lt > 2 && lt / 2 >= L) continue;
         if (pencil_smem<T>(M, lt, key.kind) > 227 * 1024) continue;
-        for (int v : fixed_variants(prec, key.kind, lt, p->ax[key.axis])) key.cand.push_back({prec, key.kind, M, L, lt, v});
+        for (int v : fixed_variants(prec, key.kind, lt, p->ax[key.axis], pair_ok(pa[q])))
+          key.cand.push_back({prec, key.kind, M, L, lt, v});
         key.cand.push_back({prec, key.kind, M, L, lt, -1});
       }
       key.ms.assign(key.cand.size(), 0.0);
@@ -540,6 +556,17 @@ int bdda_tune_pass_get(int prec, int kind, int M, int L, int* lt, int* variant) 
   const PassTune t = pass_tune(prec, kind, M, L);
   *lt = t.lt;
   *variant = t.variant;
+  return BDDA_OK;
+}
+
+int bdda_tune_pass_variants(const bdda_plan* plan, int prec, int kind, int axis, int lt, int* variants, int cap,
+                            int* n) {
+  if (!plan || !n || prec < 0 || prec > 1 || kind < 0 || kind > 2 || axis < 0 || axis > 2 || cap < 0 ||
+      (cap > 0 && !variants))
+    return BDDA_BAD_ARG;
+  const std::vector<int> v = fixed_variants(prec, kind, lt, plan->ax[axis], true);
+  *n = (int)v.size();
+  for (int i = 0; i < (int)v.size() && i < cap; ++i) variants[i] = v[i];
   return BDDA_OK;
 }
 

@@ -428,12 +428,15 @@ struct FixedKernel {
   int variant;         // id for the autotuner: minb (256 threads) or minb + 16 * threads / 32
   int r[4];            // radix sequence, padded with 1
   FixedLaunchFn fn;
+  int pair;            // 1: column-pair jobs (needs even L and 16-byte aligned fields)
 };
 const FixedKernel* fixed_table_a(int* n);
 const FixedKernel* fixed_table_b(int* n);
 const FixedKernel* fixed_table_c(int* n);
 const FixedKernel* fixed_table_d(int* n);
 const FixedKernel* fixed_table_e(int* n);
+const FixedKernel* fixed_table_f(int* n);
+const FixedKernel* fixed_table_g(int* n);
 
 
 }  // namespace bdda

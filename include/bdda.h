@@ -91,10 +91,17 @@ int bdda_tune_get(int prec, int kind, size_t* smem_budget, int* threads);
  * at block width L: column tile width lt (2, 4, 8; 0 = the smem_budget rule)
  * and kernel variant (0 = the first specialised kernel compiled for the radix
  * sequence; k in 1..8 = the one of 256 threads compiled for k resident CTAs
- * per SM; k + 16 * (threads / 32) = the one of that CTA size; -1 = the
- * generic run-time-radix kernel).  Process-wide; set by bdda_autotune. */
+ * per SM; k + 16 * (threads / 32) = the one of that CTA size; 512 + either
+ * = a complex64 kernel whose jobs take two adjacent columns, used when L is
+ * even and the pass's field pointers are 16-byte aligned; -1 = the generic
+ * run-time-radix kernel).  Process-wide; set by bdda_autotune. */
 int bdda_tune_pass(int prec, int kind, int M, int L, int lt, int variant);
 int bdda_tune_pass_get(int prec, int kind, int M, int L, int* lt, int* variant);
+/* Variant ids (as bdda_tune_pass) of the specialised kernels compiled for the
+ * pass (prec, kind) over this plan's axis (0 = x, 1 = y, 2 = z) at tile width
+ * lt: up to cap of them into variants, their number into *n. */
+int bdda_tune_pass_variants(const bdda_plan* plan, int prec, int kind, int axis, int lt, int* variants, int cap,
+                            int* n);
 /* Autotuner (no counterpart in the reference; the reference's scipy.fft plans
  * itself).  Runs block MVPs of this plan on the caller's buffers (arguments as
  * bdda_block_mvp; out and work are overwritten), times each pass over every

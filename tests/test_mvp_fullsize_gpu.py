@@ -87,3 +87,35 @@ def test_autotuned_launch_choices_keep_the_product(case, prec):
     Y1 = _mvp(case, prec, case["S"])
     tol = 1e-12 if prec == 0 else 2e-5
     assert (Y1 - Y0).abs().max().item() / Y0.abs().max().item() < tol
+
+
+def test_every_compiled_complex64_variant_gives_the_product(case):
+    """Each specialised complex64 kernel of each pass (one-column and
+    column-pair jobs, every CTA size and register bound), forced in turn,
+    gives the product of the pass's generic kernel: the pair kernels run the
+    one-column arithmetic on 16-byte accesses, so the difference stays at
+    the level of the generic kernel's own rounding (<= 1e-6 relative)."""
+    import ctypes as C
+    lib = case["lib"].load()
+    plan = case["plan"]
+    Y0 = _mvp(case, 1, case["S"])
+    scale = Y0.abs().max().item()
+    tested = 0
+    try:
+        for kind, axis in ((0, 2), (0, 1), (1, 0), (2, 1), (2, 2)):
+            M = plan.m[axis]
+            buf, n = (C.c_int * 64)(), C.c_int()
+            assert lib.bdda_tune_pass_variants(plan.handle, 1, kind, axis, 8, buf, 64, C.byref(n)) == 0
+            variants = list(buf[:n.value])
+            assert any(v >= 512 for v in variants), (kind, axis, variants)
+            for v in variants + [-1]:
+                assert lib.bdda_tune_pass(1, kind, M, 64, 8, v) == 0
+                Y = _mvp(case, 1, case["S"])
+                err = (Y - Y0).abs().max().item() / scale
+                assert err < 1e-6, (kind, axis, v, err)
+                tested += 1
+            assert lib.bdda_tune_pass(1, kind, M, 64, 0, 0) == 0
+    finally:
+        for kind, axis in ((0, 2), (0, 1), (1, 0), (2, 1), (2, 2)):
+            lib.bdda_tune_pass(1, kind, plan.m[axis], 64, 0, 0)
+    assert tested >= 20
