@@ -17,7 +17,7 @@
 // Modes: complex128; complex64; and the mixed form of bdda_mixed_solve
 // (complex128 vectors, Gram products and L x L steps, complex64 products
 // inside the iteration, the residual replaced by the complex128 true residual
-// M^-1 (B - A X) after every 100-fold drop and before stopping, warm
+// M^-1 (B - A X) after every 10-fold drop (bdda_tune_mixed) and before stopping, warm
 // restarts while the true residual is above tol).
 //
 // The pencil passes use the generic run-time-radix kernel body (problems
@@ -44,7 +44,6 @@ constexpr int kClsBlas = 5;
 constexpr int kCheckEvery = 4;    // iterations between host reads of the active count
 constexpr int kRowsPerBlasItem = 512;
 constexpr size_t kPencilBudget = 80 * 1024;
-constexpr double kReplaceDrop = 1e-2;   // mixed form: replace the residual after a 100-fold drop
 constexpr double kDivergeFactor = 1e3;  // mixed form: abandon when the residual exceeds its minimum so far by this
 
 // ---- device work list -------------------------------------------------------
@@ -301,6 +300,7 @@ struct Outs {
   int itermax;
   double tol;
   // mixed form
+  double replace_drop;   // replace the residual after this drop (the one-problem solver's setting)
   double* prev;      // [nprob] true residual of the previous round
   int* total;        // [nprob] iterations of all rounds so far
   int* ran;          // [nprob] iterations of the last round; -1 breakdown
@@ -348,7 +348,7 @@ __global__ void batch_check_kernel(const ProbDev* pd, int* flags, int* left, con
     } else {
       o.ran[p] = k + 1;
       const double rm = k == 0 ? 0.0 : o.rmax[p];
-      if (bad != 2 && err == err && (err < o.tol || err < kReplaceDrop * rm)) {
+      if (bad != 2 && err == err && (err < o.tol || err < o.replace_drop * rm)) {
         o.repl[p] = 1;   // the replacement step decides
       } else {
         if (o.hist && tot + k < o.itermax) o.hist[(int64_t)p * o.itermax + tot + k] = err;
@@ -803,6 +803,7 @@ int batch_run(const bdda_batch_problem* pr, int nprob, int mode, int L, double t
   o.hist = history ? reinterpret_cast<double*>(w + lay.hist) : nullptr;
   o.itermax = std::max(itermax, 1);
   o.tol = tol;
+  o.replace_drop = mixed_replace_drop();
   o.prev = reinterpret_cast<double*>(w + lay.prev);
   o.total = reinterpret_cast<int*>(w + lay.totalit);
   o.ran = reinterpret_cast<int*>(w + lay.ran);

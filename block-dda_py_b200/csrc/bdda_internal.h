@@ -46,6 +46,9 @@ inline const T* table_ptr(const bdda_plan* p, size_t off) {
   return reinterpret_cast<const T*>(static_cast<const unsigned char*>(p->dev_tables) + off);
 }
 
+// Residual replacement drop of the mixed-form BiCGSTAB (bdda_tune_mixed).
+double mixed_replace_drop();
+
 // Launch the block MVP in one precision (defined in bdda_mvp.cu).
 template <typename T>
 int block_mvp_impl(const bdda_plan* plan, int L, const T* ghat, const int32_t* cell_map,

@@ -296,7 +296,14 @@ static int read_state(Ctx<T>& c, double* err, int* bad) {
 // Residual replacement in the mixed form: when the recursive residual has
 // dropped by this factor below its largest value since the last replacement
 // (or below tol), it is recomputed from X with the complex128 product.
-constexpr double kReplaceDrop = 1e-2;
+// Once the true residual is below g_mixed_switch * tol the remaining
+// iterations use complex128 products: near tol the complex64 rounding of the
+// products, not the Krylov space, limits the recursion (0 = never switch).
+// Both set by bdda_tune_mixed.
+static double g_replace_drop = 1e-1;
+static double g_mixed_switch = 0.0;
+
+double mixed_replace_drop() { return g_replace_drop; }
 // ... and it is abandoned as diverged once the residual exceeds its smallest
 // value so far by this factor (block-BiCGSTAB on strongly scattering
 // particles can amplify the complex64 rounding of the products without bound).
@@ -349,7 +356,7 @@ static int bicgstab_core(Ctx<T>& c, bool has_x0, double tol, int itermax, int* i
     int bad = 0;
     TRY(read_state(c, &err, &bad));
     if (bad == 1) return BDDA_BREAKDOWN;
-    if (bad != 2 && c.ghat32 && (err < tol || err < kReplaceDrop * rmax)) {
+    if (bad != 2 && c.ghat32 && (err < tol || err < g_replace_drop * rmax || err < g_mixed_switch * tol)) {
       // complex64 products: replace the recursive residual by the true one
       // (complex128 product; Z is free until the next iteration), so the
       // drift of the recursion stays at the level of the current residual
@@ -360,6 +367,7 @@ static int bicgstab_core(Ctx<T>& c, bool has_x0, double tol, int itermax, int* i
       BDDA_CUDA_TRY(cudaGetLastError());
       TRY(read_state(c, &err, &bad));
       rmax = err;
+      if (err < g_mixed_switch * tol) c.ghat32 = nullptr;   // complex128 products from here on
     }
     rmax = err > rmax ? err : rmax;
     rmin = err < rmin ? err : rmin;
@@ -805,7 +813,12 @@ static int run_refine(int solver, bool restart, const bdda_plan* p, int L, int n
 // product and L x L step in complex128 and computes the products inside the
 // iteration in complex64 (the product dominates the cost).  BiCGSTAB replaces
 // its recursive residual by the true one (complex128 product) whenever it
-// has dropped 100-fold and before it stops; COCG-rq runs its recursion to
+// has dropped 10-fold (bdda_tune_mixed) and before it stops.  Under 1e-7
+// perturbations of B, a 100-fold interval let the drift of the recursion
+// swing the iteration count of the x=20 particle between 20 and 62
+// (complex128: 19) and of a strongly scattering x=9.2 one between 111 and
+// 138 (complex128: 86-90); a 10-fold one keeps them at 19-22 and 106-120.
+// COCG-rq runs its recursion to
 // kInnerFrac * tol.  Then the true residual M^-1 (B - A X) decides; if it is
 // not below tol the solver restarts from the current X (warm start).  A
 // BiCGSTAB recursion that diverges under the complex64 products is abandoned
@@ -1010,6 +1023,20 @@ int bdda_refine_solve(const bdda_plan* p, int solver, int L, int n_occ, const vo
                     static_cast<const double2*>(B), static_cast<const double2*>(X0), tol, itermax, inner_tol,
                     max_outer, static_cast<double2*>(X), iter_fin, err_fin, history, work, work_bytes,
                     (cudaStream_t)stream);
+}
+
+int bdda_tune_mixed(double replace_drop, double switch_ratio) {
+  if (!(replace_drop > 0.0 && replace_drop < 1.0) || !(switch_ratio >= 0.0)) return BDDA_BAD_ARG;
+  g_replace_drop = replace_drop;
+  g_mixed_switch = switch_ratio;
+  return BDDA_OK;
+}
+
+int bdda_tune_mixed_get(double* replace_drop, double* switch_ratio) {
+  if (!replace_drop || !switch_ratio) return BDDA_BAD_ARG;
+  *replace_drop = g_replace_drop;
+  *switch_ratio = g_mixed_switch;
+  return BDDA_OK;
 }
 
 size_t bdda_mixed_workspace_bytes(const bdda_plan* p, int L, int n_occ) {

@@ -233,12 +233,23 @@ int bdda_refine_solve(const bdda_plan* plan, int solver, int L, int n_occ, const
  * reference) ------------------------------------------------------------------
  * The block solver of `solver` with X, the residual, every Krylov vector,
  * Gram product and L x L step in complex128, and the products inside the
- * iteration in complex64 (ghat_c64 from bdda_green_convert).  The recursion
- * runs to tol / 2; the true residual ||M^-1 (B - A X)|| / ||M^-1 B|| from the
- * complex128 product then decides, and the solver restarts from X (exact
- * product) while it is not below tol, up to max_outer rounds.  err_fin is
- * that true residual; iter_fin counts the iterations of all rounds. */
+ * iteration in complex64 (ghat_c64 from bdda_green_convert).  BiCGSTAB
+ * replaces its recursive residual by the true one ||M^-1 (B - A X)|| /
+ * ||M^-1 B|| (complex128 product) after every replace_drop-fold drop and
+ * before it stops, and finishes with complex128 products once the true
+ * residual is below switch_ratio * tol (bdda_tune_mixed); a recursion that
+ * diverges is abandoned for complex128 products from the start.  COCG-rq's
+ * recursion runs to tol / 2 and the true residual then decides.  The solver
+ * restarts from X (exact product) while the true residual is not below tol,
+ * up to max_outer rounds.  err_fin is the final residual (the true one, or
+ * after a switch the complex128 recursion's); iter_fin counts the iterations
+ * of all rounds. */
 size_t bdda_mixed_workspace_bytes(const bdda_plan* plan, int L, int n_occ);
+/* Process-wide settings of bdda_mixed_solve's BiCGSTAB (and of the batched
+ * solver's mode MIXED for replace_drop): replace_drop in (0, 1), default
+ * 0.1; switch_ratio >= 0, default 0 (complex64 products to the end). */
+int bdda_tune_mixed(double replace_drop, double switch_ratio);
+int bdda_tune_mixed_get(double* replace_drop, double* switch_ratio);
 int bdda_mixed_solve(const bdda_plan* plan, int solver, int L, int n_occ, const void* ghat_c128,
                      const void* ghat_c64, const int32_t* cell_map, const void* diag, const void* B,
                      const void* X0, double tol, int itermax, int max_outer, void* X, int* iter_fin,
