@@ -268,6 +268,7 @@ __global__ void __launch_bounds__(NT, MINB) fixed_pencil_kernel(const PassArgs a
 
 template <typename T, int KIND, int LT, int MINB, int NT, int PAIR, int R0, int R1, int R2, int R3>
 int fixed_launch(const PassArgs& a0, int64_t P0, cudaStream_t st) {
+  static_assert(NT % 32 == 0 && NT <= 512 && MINB >= 1 && MINB < 16, "variant id encodes whole warps and MINB < 16");
   using RS = RadixSeq<R0, R1, R2, R3>;
   PassArgs a = a0;
   if (a.ax.M != RS::M) return BDDA_BAD_ARG;
@@ -288,8 +289,8 @@ int fixed_launch(const PassArgs& a0, int64_t P0, cudaStream_t st) {
 
 // Table entry of a specialised kernel with 256 threads per CTA (variant id =
 // MINB) or NT threads (variant id = MINB + 16 NT/32: the CTA size that makes
-// the stages' butterfly jobs fill whole rounds of threads); column-pair
-// kernels add 512 to the id.
+// the stages' butterfly jobs fill whole rounds of threads; NT a multiple of
+// 32, so that ids stay distinct); column-pair kernels add 512 to the id.
 #define BDDA_FIXED(T, PREC, KIND, LT, MINB, R0, R1, R2, R3) \
   { PREC, KIND, LT, MINB, MINB, {R0, R1, R2, R3}, &fixed_launch<T, KIND, LT, MINB, 256, 0, R0, R1, R2, R3>, 0 }
 #define BDDA_FIXED_NT(T, PREC, KIND, LT, MINB, NT, R0, R1, R2, R3)                              \

@@ -147,3 +147,31 @@ def test_mixed_settings_round_trip_and_reject_bad_values():
         assert lib.bdda_tune_mixed_get(None, C.byref(s)) == _lib.BAD_ARG
     finally:
         lib.bdda_tune_mixed(d0, s0)
+
+
+def test_pass_variant_lists_name_the_compiled_kernels():
+    """Host-only: for the x=20 particle's grid (192 x 224 x 350) every complex64
+    pass has one-column and column-pair (id >= 512) specialised kernels at
+    tile width 8, complex128 only one-column ones; the count is reported even
+    when cap is 0; bad arguments are rejected."""
+    lib = _lib.load()
+    h = C.c_void_p()
+    assert lib.bdda_plan_create((C.c_int * 3)(93, 112, 174), None, C.byref(h)) == 0
+    try:
+        m = (C.c_int * 3)()
+        assert lib.bdda_plan_grid(h, m) == 0 and list(m) == [192, 224, 350]
+        buf, n = (C.c_int * 64)(), C.c_int()
+        for kind, axis in ((0, 2), (0, 1), (1, 0), (2, 1), (2, 2)):
+            assert lib.bdda_tune_pass_variants(h, 1, kind, axis, 8, buf, 64, C.byref(n)) == 0
+            ids = list(buf[:n.value])
+            assert any(v >= 512 for v in ids) and any(0 < v < 512 for v in ids), (kind, axis, ids)
+            assert len(set(ids)) == len(ids)
+            assert lib.bdda_tune_pass_variants(h, 1, kind, axis, 8, None, 0, C.byref(n)) == 0 and n.value == len(ids)
+            assert lib.bdda_tune_pass_variants(h, 0, kind, axis, 4, buf, 64, C.byref(n)) == 0
+            ids = list(buf[:n.value])
+            assert ids and all(v < 512 for v in ids) and len(set(ids)) == len(ids), (kind, axis, ids)
+        assert lib.bdda_tune_pass_variants(h, 1, 3, 0, 8, buf, 64, C.byref(n)) == _lib.BAD_ARG
+        assert lib.bdda_tune_pass_variants(h, 1, 1, 3, 8, buf, 64, C.byref(n)) == _lib.BAD_ARG
+        assert lib.bdda_tune_pass_variants(None, 1, 1, 0, 8, buf, 64, C.byref(n)) == _lib.BAD_ARG
+    finally:
+        lib.bdda_plan_destroy(h)
