@@ -505,31 +505,36 @@ def run_sweep(args):
     torch.cuda.synchronize()
     green_s = time.perf_counter() - t0
 
-    def arm(batched, precision):
-        for d in dds:
+    def arm(batched, precision, idx=None):
+        idx = range(len(dds)) if idx is None else idx
+        ds, gs = [dds[i] for i in idx], [greens[i] for i in idx]
+        for d in ds:
             d.precision = precision
         torch.cuda.synchronize()
         n0 = lib.bdda_launch_count()
         t0 = time.perf_counter()
-        for d, g in zip(dds, greens):
+        for d, g in zip(ds, gs):
             d.set_interaction_matrix(green=g)
         if batched:
-            sc.solve_matrix_equations(dds)
+            sc.solve_matrix_equations(ds)
         else:
-            for d in dds:
+            for d in ds:
                 d.solve_matrix_equation()
-        obs = [d.observables() for d in dds]
+        obs = [d.observables() for d in ds]
         torch.cuda.synchronize()
         dt = time.perf_counter() - t0
-        return dict(value=round(len(dds) * L / dt, 2), seconds=round(dt, 3),
+        return dict(value=round(len(ds) * L / dt, 2), seconds=round(dt, 3),
                     launches=int(lib.bdda_launch_count() - n0),
-                    converged=int(sum(d.converge for d in dds)),
-                    iterations_mean=round(float(np.mean([d.iter_fin + 1 for d in dds])), 2)), obs
+                    converged=int(sum(d.converge for d in ds)),
+                    iterations_mean=round(float(np.mean([d.iter_fin + 1 for d in ds])), 2)), obs
 
     arms = [a for a in args.sweep_arms.split(",") if a]
     table = {"one_at_a_time_fp64": (False, None), "one_at_a_time_mixed": (False, "mixed"),
              "batched_fp64": (True, None), "batched_mixed": (True, "mixed")}
-    arm(True, None)                         # warm-up (graphs, kernels, allocator)
+    # warm-up (graphs, kernels, allocator) on the smallest problems, every requested form
+    small = sorted(range(len(dds)), key=lambda i: n_dip[i // len(SWEEP_WL)])[:6]
+    for name in arms:
+        arm(table[name][0], table[name][1], small)
     res = {}
     obs = {}
     for name in arms:

@@ -44,7 +44,6 @@ constexpr int kClsBlas = 5;
 constexpr int kCheckEvery = 4;    // iterations between host reads of the active count
 constexpr int kRowsPerBlasItem = 512;
 constexpr size_t kPencilBudget = 80 * 1024;
-constexpr double kDivergeFactor = 1e3;  // mixed form: abandon when the residual exceeds its minimum so far by this
 
 // ---- device work list -------------------------------------------------------
 struct ListDev {
@@ -300,7 +299,8 @@ struct Outs {
   int itermax;
   double tol;
   // mixed form
-  double replace_drop;   // replace the residual after this drop (the one-problem solver's setting)
+  double replace_drop;     // replace the residual after this drop (the one-problem solver's setting)
+  double diverge_factor;   // abandon when the residual exceeds its minimum so far by this (same)
   double* prev;      // [nprob] true residual of the previous round
   int* total;        // [nprob] iterations of all rounds so far
   int* ran;          // [nprob] iterations of the last round; -1 breakdown
@@ -356,7 +356,7 @@ __global__ void batch_check_kernel(const ProbDev* pd, int* flags, int* left, con
         const double rn = k == 0 ? err : fmin(o.rmin[p], err);
         o.rmin[p] = rn;
         if (bad == 2 || !(err < INFINITY) || tot + k + 1 >= o.itermax) stop = true;
-        if (err > kDivergeFactor * rn) {   // diverged: the problem stops unconverged
+        if (err > o.diverge_factor * rn) {   // diverged: the problem stops unconverged
           o.ran[p] = -2;
           stop = true;
         }
@@ -804,6 +804,7 @@ int batch_run(const bdda_batch_problem* pr, int nprob, int mode, int L, double t
   o.itermax = std::max(itermax, 1);
   o.tol = tol;
   o.replace_drop = mixed_replace_drop();
+  o.diverge_factor = mixed_diverge_factor();
   o.prev = reinterpret_cast<double*>(w + lay.prev);
   o.total = reinterpret_cast<int*>(w + lay.totalit);
   o.ran = reinterpret_cast<int*>(w + lay.ran);

@@ -46,8 +46,10 @@ inline const T* table_ptr(const bdda_plan* p, size_t off) {
   return reinterpret_cast<const T*>(static_cast<const unsigned char*>(p->dev_tables) + off);
 }
 
-// Residual replacement drop of the mixed-form BiCGSTAB (bdda_tune_mixed).
+// Residual replacement drop and divergence factor of the mixed-form
+// BiCGSTAB (bdda_tune_mixed).
 double mixed_replace_drop();
+double mixed_diverge_factor();
 
 // Launch the block MVP in one precision (defined in bdda_mvp.cu).
 template <typename T>

@@ -229,6 +229,8 @@ struct Ctx {
   const float2* ghat32 = nullptr;
   float2 *diag32 = nullptr, *jpre32 = nullptr, *in32 = nullptr, *out32 = nullptr;
   bool diverged = false;   // set when the complex64-product recursion blew up
+  T* xbest = nullptr;      // mixed form: X at the smallest residual so far (or null)
+  double best = INFINITY;  // that residual
 };
 
 // The product in the vectors' own precision.
@@ -306,8 +308,15 @@ static double g_mixed_switch = 0.0;
 double mixed_replace_drop() { return g_replace_drop; }
 // ... and it is abandoned as diverged once the residual exceeds its smallest
 // value so far by this factor (block-BiCGSTAB on strongly scattering
-// particles can amplify the complex64 rounding of the products without bound).
-constexpr double kDivergeFactor = 1e3;
+// particles can amplify the complex64 rounding of the products without bound;
+// bdda_tune_mixed).  The fallback continues from the best X so far, so an
+// early call costs little: on a sweep of 48 strongly scattering problems
+// (m = 1.53) a factor of 10 took the mixed form from 11.3 to 16.2
+// orientations/s (complex128: 17.1), against 1000 before.  Block BiCGSTAB's
+// residual rises up to ~4-fold on the way down on the x=20 particle.
+static double g_diverge_factor = 10.0;
+
+double mixed_diverge_factor() { return g_diverge_factor; }
 
 // Block-BiCGSTAB (bl_krylov.py:121-187).  vec: 0 X, 1 R, 2 P, 3 R0, 4 V, 5 T, 6 Z, 7 Bj
 template <typename T>
@@ -370,13 +379,17 @@ static int bicgstab_core(Ctx<T>& c, bool has_x0, double tol, int itermax, int* i
       if (err < g_mixed_switch * tol) c.ghat32 = nullptr;   // complex128 products from here on
     }
     rmax = err > rmax ? err : rmax;
+    if (c.xbest && c.ghat32 && bad == 0 && err < c.best) {   // keep X for a warm fallback
+      BDDA_CUDA_TRY(cudaMemcpyAsync(c.xbest, X, (size_t)c.n * L * sizeof(T), cudaMemcpyDeviceToDevice, c.stream));
+      c.best = err;
+    }
     rmin = err < rmin ? err : rmin;
     if (hist) hist[k] = err;
     *iter_fin = k;
     *err_fin = err;
     if (bad == 2) return BDDA_NOT_CONVERGED;   // NaN/Inf reached: stop, reported as not converged
     if (err < tol) return BDDA_OK;
-    if (c.ghat32 && err > kDivergeFactor * rmin) {
+    if (c.ghat32 && err > g_diverge_factor * rmin) {
       c.diverged = true;
       return BDDA_NOT_CONVERGED;
     }
@@ -822,12 +835,14 @@ static int run_refine(int solver, bool restart, const bdda_plan* p, int L, int n
 // kInnerFrac * tol.  Then the true residual M^-1 (B - A X) decides; if it is
 // not below tol the solver restarts from the current X (warm start).  A
 // BiCGSTAB recursion that diverges under the complex64 products is abandoned
-// and the problem solved again with complex128 products.
+// and the problem solved on with complex128 products, warm-started from the X
+// of the smallest residual the recursion reached (kept in xbest) when that
+// is below the zero start's.
 constexpr double kInnerFrac = 0.5;
 
 struct MLayout {
   Layout base;
-  size_t in32, out32, diag32, jpre32, total;
+  size_t in32, out32, diag32, jpre32, xbest, total;
 };
 
 static MLayout mlayout(const bdda_plan* p, int L, int n_occ) {
@@ -839,6 +854,7 @@ static MLayout mlayout(const bdda_plan* p, int L, int n_occ) {
   o.out32 = off; off = al(off + v32);
   o.diag32 = off; off = al(off + (size_t)3 * n_occ * 8);
   o.jpre32 = off; off = al(off + (size_t)3 * n_occ * 8);
+  o.xbest = off; off = al(off + (size_t)3 * n_occ * L * 16);
   o.total = off;
   return o;
 }
@@ -866,6 +882,7 @@ static int run_mixed(int solver, const bdda_plan* p, int L, int n_occ, const voi
   const int64_t ne = c.n * L;
   // vec: 0 X, 1 R, 4 V, 7 Bj (the solver cores' roles)
   double2 *X = c.vec[0], *R = c.vec[1], *V = c.vec[4], *Bj = c.vec[7];
+  if (solver == BDDA_BICGSTAB) c.xbest = reinterpret_cast<double2*>(w + o.xbest);
   BDDA_CUDA_TRY(cudaMemsetAsync(c.st, 0, sizeof(SolverState), st));
   constants_kernel<<<1, 32, 0, st>>>(c.sp);
   prepare_kernel<double2><<<kRedBlocks, 256, 0, st>>>(diag, B, c.n, L, c.diag, c.jpre, Bj);
@@ -898,14 +915,20 @@ static int run_mixed(int solver, const bdda_plan* p, int L, int n_occ, const voi
     if (s_in != BDDA_OK && s_in != BDDA_NOT_CONVERGED) return s_in;
     total += it_in + 1;
     *iter_fin = total - 1;
-    if (c.diverged) {   // give up the complex64 products: complex128 from the start
+    if (c.diverged) {   // give up the complex64 products: complex128 from the best X so far
       c.diverged = false;
       c.ghat32 = nullptr;
-      if (X0) BDDA_CUDA_TRY(cudaMemcpyAsync(X, X0, (size_t)ne * sizeof(double2), cudaMemcpyDeviceToDevice, st));
-      else BDDA_CUDA_TRY(cudaMemsetAsync(X, 0, (size_t)ne * sizeof(double2), st));
+      const bool from_best = c.best < 1.0;   // the recursion got below the zero start's residual
+      if (from_best) {
+        BDDA_CUDA_TRY(cudaMemcpyAsync(X, c.xbest, (size_t)ne * sizeof(double2), cudaMemcpyDeviceToDevice, st));
+      } else if (X0) {
+        BDDA_CUDA_TRY(cudaMemcpyAsync(X, X0, (size_t)ne * sizeof(double2), cudaMemcpyDeviceToDevice, st));
+      } else {
+        BDDA_CUDA_TRY(cudaMemsetAsync(X, 0, (size_t)ne * sizeof(double2), st));
+      }
       if (total < itermax) {
-        const int s64 = bicgstab_core<double2>(c, X0 != nullptr, tol, itermax - total, &it_in, &err_in,
-                                               hist ? hist + total : nullptr);
+        const int s64 = bicgstab_core<double2>(c, from_best || X0 != nullptr, tol, itermax - total, &it_in,
+                                               &err_in, hist ? hist + total : nullptr);
         if (s64 != BDDA_OK && s64 != BDDA_NOT_CONVERGED) return s64;
         total += it_in + 1;
         *iter_fin = total - 1;
@@ -1025,17 +1048,20 @@ int bdda_refine_solve(const bdda_plan* p, int solver, int L, int n_occ, const vo
                     (cudaStream_t)stream);
 }
 
-int bdda_tune_mixed(double replace_drop, double switch_ratio) {
-  if (!(replace_drop > 0.0 && replace_drop < 1.0) || !(switch_ratio >= 0.0)) return BDDA_BAD_ARG;
+int bdda_tune_mixed(double replace_drop, double switch_ratio, double diverge_factor) {
+  if (!(replace_drop > 0.0 && replace_drop < 1.0) || !(switch_ratio >= 0.0) || !(diverge_factor > 1.0))
+    return BDDA_BAD_ARG;
   g_replace_drop = replace_drop;
   g_mixed_switch = switch_ratio;
+  g_diverge_factor = diverge_factor;
   return BDDA_OK;
 }
 
-int bdda_tune_mixed_get(double* replace_drop, double* switch_ratio) {
-  if (!replace_drop || !switch_ratio) return BDDA_BAD_ARG;
+int bdda_tune_mixed_get(double* replace_drop, double* switch_ratio, double* diverge_factor) {
+  if (!replace_drop || !switch_ratio || !diverge_factor) return BDDA_BAD_ARG;
   *replace_drop = g_replace_drop;
   *switch_ratio = g_mixed_switch;
+  *diverge_factor = g_diverge_factor;
   return BDDA_OK;
 }
 

@@ -238,7 +238,8 @@ int bdda_refine_solve(const bdda_plan* plan, int solver, int L, int n_occ, const
  * ||M^-1 B|| (complex128 product) after every replace_drop-fold drop and
  * before it stops, and finishes with complex128 products once the true
  * residual is below switch_ratio * tol (bdda_tune_mixed); a recursion that
- * diverges is abandoned for complex128 products from the start.  COCG-rq's
+ * diverges is abandoned for complex128 products, warm-started from the X of
+ * its smallest residual when that is below 1.  COCG-rq's
  * recursion runs to tol / 2 and the true residual then decides.  The solver
  * restarts from X (exact product) while the true residual is not below tol,
  * up to max_outer rounds.  err_fin is the final residual (the true one, or
@@ -246,10 +247,12 @@ int bdda_refine_solve(const bdda_plan* plan, int solver, int L, int n_occ, const
  * of all rounds. */
 size_t bdda_mixed_workspace_bytes(const bdda_plan* plan, int L, int n_occ);
 /* Process-wide settings of bdda_mixed_solve's BiCGSTAB (and of the batched
- * solver's mode MIXED for replace_drop): replace_drop in (0, 1), default
- * 0.1; switch_ratio >= 0, default 0 (complex64 products to the end). */
-int bdda_tune_mixed(double replace_drop, double switch_ratio);
-int bdda_tune_mixed_get(double* replace_drop, double* switch_ratio);
+ * solver's mode MIXED for replace_drop and diverge_factor): replace_drop in
+ * (0, 1), default 0.1; switch_ratio >= 0, default 0 (complex64 products to
+ * the end); diverge_factor > 1, default 10: the recursion counts as
+ * diverged once its residual exceeds its smallest value so far by this. */
+int bdda_tune_mixed(double replace_drop, double switch_ratio, double diverge_factor);
+int bdda_tune_mixed_get(double* replace_drop, double* switch_ratio, double* diverge_factor);
 int bdda_mixed_solve(const bdda_plan* plan, int solver, int L, int n_occ, const void* ghat_c128,
                      const void* ghat_c64, const int32_t* cell_map, const void* diag, const void* B,
                      const void* X0, double tol, int itermax, int max_outer, void* X, int* iter_fin,

@@ -131,22 +131,24 @@ def test_batch_workspace_query_checks_arguments():
 
 
 def test_mixed_settings_round_trip_and_reject_bad_values():
-    """Host-only: bdda_tune_mixed sets the mixed BiCGSTAB's replacement drop and
-    complex128 switch, keeps them on bad values, and bdda_tune_mixed_get reads them."""
+    """Host-only: bdda_tune_mixed sets the mixed BiCGSTAB's replacement drop,
+    complex128 switch and divergence factor, keeps them on bad values, and
+    bdda_tune_mixed_get reads them."""
     lib = _lib.load()
-    d, s = C.c_double(), C.c_double()
-    assert lib.bdda_tune_mixed_get(C.byref(d), C.byref(s)) == 0
-    d0, s0 = d.value, s.value
-    assert d0 == 0.1 and s0 == 0.0
+    d, s, f = C.c_double(), C.c_double(), C.c_double()
+    get = lambda: (lib.bdda_tune_mixed_get(C.byref(d), C.byref(s), C.byref(f)), d.value, s.value, f.value)
+    rc, d0, s0, f0 = get()
+    assert rc == 0 and (d0, s0, f0) == (0.1, 0.0, 10.0)
     try:
-        assert lib.bdda_tune_mixed(0.05, 10.0) == 0
-        assert lib.bdda_tune_mixed_get(C.byref(d), C.byref(s)) == 0 and (d.value, s.value) == (0.05, 10.0)
-        for bad in ((0.0, 0.0), (1.0, 0.0), (0.1, -1.0), (float("nan"), 0.0)):
+        assert lib.bdda_tune_mixed(0.05, 10.0, 50.0) == 0
+        assert get() == (0, 0.05, 10.0, 50.0)
+        for bad in ((0.0, 0.0, 10.0), (1.0, 0.0, 10.0), (0.1, -1.0, 10.0), (float("nan"), 0.0, 10.0),
+                    (0.1, 0.0, 1.0), (0.1, 0.0, float("nan"))):
             assert lib.bdda_tune_mixed(*bad) == _lib.BAD_ARG
-        assert lib.bdda_tune_mixed_get(C.byref(d), C.byref(s)) == 0 and (d.value, s.value) == (0.05, 10.0)
-        assert lib.bdda_tune_mixed_get(None, C.byref(s)) == _lib.BAD_ARG
+        assert get() == (0, 0.05, 10.0, 50.0)
+        assert lib.bdda_tune_mixed_get(None, C.byref(s), C.byref(f)) == _lib.BAD_ARG
     finally:
-        lib.bdda_tune_mixed(d0, s0)
+        lib.bdda_tune_mixed(d0, s0, f0)
 
 
 def test_pass_variant_lists_name_the_compiled_kernels():

@@ -217,6 +217,42 @@ def test_reliable_update_variant_small_block(mods):
     assert it + 1 <= 2 * (int(rec["bicgstab_tol5_iter_fin"]) + 1)
 
 
+def test_mixed_fallback_after_divergence_warm_starts_from_the_best_iterate(mods):
+    """With a divergence factor of 1.2 the mixed recursion counts as diverged at
+    its first 1.2-fold residual rise (x=20 particle, 16 orientations: block
+    BiCGSTAB's residual is not monotone there).  The complex128 fallback then
+    starts from the X of the smallest residual so far: the solve converges to
+    tol on the true residual, to the complex128 solution, and needs no more
+    iterations in all than a complex128 solve from zero plus the recursion's."""
+    from bdda_b200 import _lib
+    mf, bk = mods
+    rec = load_geometry(os.path.join(GOLDEN, "geometry_cfg2.npz"))
+    rec = dict(rec, euler=rec["euler"][:16])
+    n, lf, address, pos, geom, eper_r, diag, B = _case(rec)
+    til = mf.fft_init(n, 3, lf, geom["k"])
+    h64 = []
+    X64, it64, err64 = bk.bl_bicgstab_jacobi_mvp_fft(n, 3, address, til, diag, B, 1e-5, 400, history=h64)
+    lib = _lib.load()
+    import ctypes as C
+    d, sw, f = C.c_double(), C.c_double(), C.c_double()
+    assert lib.bdda_tune_mixed_get(C.byref(d), C.byref(sw), C.byref(f)) == 0
+    hm = []
+    try:
+        assert lib.bdda_tune_mixed(d.value, sw.value, 1.2) == 0
+        Xm, itm, errm = bk.bl_bicgstab_jacobi_mvp_fft(n, 3, address, til, diag, B, 1e-5, 400, precision="mixed",
+                                                      history=hm)
+    finally:
+        lib.bdda_tune_mixed(d.value, sw.value, f.value)
+    k_div = next(k for k in range(1, len(hm)) if hm[k] > 1.2 * min(hm[:k]))   # the fallback ran
+    assert errm < 1e-5 and err64 < 1e-5
+    true = O.true_residual(n, 3, address, O.fft_init(n, 3, lf, geom["k"]), diag, B, Xm)
+    assert true < 1e-5
+    assert rel(Xm, X64) < 1e-3
+    assert itm + 1 <= (k_div + 1) + (it64 + 1)
+    # the complex128 phase starts below where a zero start begins
+    assert hm[k_div + 1] < h64[0]
+
+
 def test_mixed_form_converges_where_fp32_krylov_diverges(mods):
     """A strongly scattering GRE (x = 9.2, m = 1.53 + 0.005i, 34 x 65 x 69
     lattice): complex64 Krylov vectors diverge here, the mixed form (complex64
