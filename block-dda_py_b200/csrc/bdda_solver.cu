@@ -231,6 +231,7 @@ struct Ctx {
   bool diverged = false;   // set when the complex64-product recursion blew up
   T* xbest = nullptr;      // mixed form: X at the smallest residual so far (or null)
   double best = INFINITY;  // that residual
+  bool watch = false;      // apply the divergence test to complex128 products too
 };
 
 // The product in the vectors' own precision.
@@ -389,7 +390,7 @@ static int bicgstab_core(Ctx<T>& c, bool has_x0, double tol, int itermax, int* i
     *err_fin = err;
     if (bad == 2) return BDDA_NOT_CONVERGED;   // NaN/Inf reached: stop, reported as not converged
     if (err < tol) return BDDA_OK;
-    if (c.ghat32 && err > g_diverge_factor * rmin) {
+    if ((c.ghat32 || c.watch) && err > g_diverge_factor * rmin) {
       c.diverged = true;
       return BDDA_NOT_CONVERGED;
     }
@@ -915,23 +916,34 @@ static int run_mixed(int solver, const bdda_plan* p, int L, int n_occ, const voi
     if (s_in != BDDA_OK && s_in != BDDA_NOT_CONVERGED) return s_in;
     total += it_in + 1;
     *iter_fin = total - 1;
-    if (c.diverged) {   // give up the complex64 products: complex128 from the best X so far
+    if (c.diverged) {   // give up the complex64 products
       c.diverged = false;
       c.ghat32 = nullptr;
-      const bool from_best = c.best < 1.0;   // the recursion got below the zero start's residual
-      if (from_best) {
-        BDDA_CUDA_TRY(cudaMemcpyAsync(X, c.xbest, (size_t)ne * sizeof(double2), cudaMemcpyDeviceToDevice, st));
-      } else if (X0) {
-        BDDA_CUDA_TRY(cudaMemcpyAsync(X, X0, (size_t)ne * sizeof(double2), cudaMemcpyDeviceToDevice, st));
-      } else {
-        BDDA_CUDA_TRY(cudaMemsetAsync(X, 0, (size_t)ne * sizeof(double2), st));
-      }
-      if (total < itermax) {
-        const int s64 = bicgstab_core<double2>(c, from_best || X0 != nullptr, tol, itermax - total, &it_in,
-                                               &err_in, hist ? hist + total : nullptr);
+      // complex128 from the best X so far when the recursion got below the
+      // zero start's residual, watched by the same divergence test: block
+      // BiCGSTAB restarted from a residual whose columns sit at very
+      // different levels can stagnate (a 24 x 28 x 35 GRE did for 480
+      // iterations where a zero start converges in 10); then once more
+      // from the start, unwatched
+      bool warm = c.best < 1.0;
+      while (total < itermax) {
+        if (warm) {
+          BDDA_CUDA_TRY(cudaMemcpyAsync(X, c.xbest, (size_t)ne * sizeof(double2), cudaMemcpyDeviceToDevice, st));
+        } else if (X0) {
+          BDDA_CUDA_TRY(cudaMemcpyAsync(X, X0, (size_t)ne * sizeof(double2), cudaMemcpyDeviceToDevice, st));
+        } else {
+          BDDA_CUDA_TRY(cudaMemsetAsync(X, 0, (size_t)ne * sizeof(double2), st));
+        }
+        c.watch = warm;
+        const int s64 = bicgstab_core<double2>(c, warm || X0 != nullptr, tol, itermax - total, &it_in, &err_in,
+                                               hist ? hist + total : nullptr);
+        c.watch = false;
         if (s64 != BDDA_OK && s64 != BDDA_NOT_CONVERGED) return s64;
         total += it_in + 1;
         *iter_fin = total - 1;
+        if (!(warm && c.diverged)) break;
+        c.diverged = false;
+        warm = false;
       }
       max_outer = round + 1;   // this is the last round
     } else if (solver == BDDA_BICGSTAB && s_in == BDDA_OK) {

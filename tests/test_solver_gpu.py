@@ -221,9 +221,11 @@ def test_mixed_fallback_after_divergence_warm_starts_from_the_best_iterate(mods)
     """With a divergence factor of 1.2 the mixed recursion counts as diverged at
     its first 1.2-fold residual rise (x=20 particle, 16 orientations: block
     BiCGSTAB's residual is not monotone there).  The complex128 fallback then
-    starts from the X of the smallest residual so far: the solve converges to
-    tol on the true residual, to the complex128 solution, and needs no more
-    iterations in all than a complex128 solve from zero plus the recursion's."""
+    starts from the X of the smallest residual so far, watched by the same
+    test (and restarted from zero once if that trips too): the solve converges
+    to tol on the true residual, to the complex128 solution, its complex128
+    phase starts below a zero start's first residual, and it needs no more
+    iterations than the recursion plus two complex128 solves from zero."""
     from bdda_b200 import _lib
     mf, bk = mods
     rec = load_geometry(os.path.join(GOLDEN, "geometry_cfg2.npz"))
@@ -248,9 +250,40 @@ def test_mixed_fallback_after_divergence_warm_starts_from_the_best_iterate(mods)
     true = O.true_residual(n, 3, address, O.fft_init(n, 3, lf, geom["k"]), diag, B, Xm)
     assert true < 1e-5
     assert rel(Xm, X64) < 1e-3
-    assert itm + 1 <= (k_div + 1) + (it64 + 1)
+    assert itm + 1 <= (k_div + 1) + 2 * (it64 + 1)
     # the complex128 phase starts below where a zero start begins
     assert hm[k_div + 1] < h64[0]
+
+
+def test_mixed_form_recovers_where_a_warm_complex128_restart_stagnates():
+    """A small strongly scattering GRE (x = 4.4, m = 1.53 + 0.005i, 24 x 28 x 35
+    lattice, 32 orientations, built as the batched sweep builds it): the
+    complex64 recursion stagnates near 1e-3 and counts as diverged; a
+    complex128 restart from its best X stagnated for 480 iterations, so that
+    restart is watched and replaced by a zero start.  The mixed solve converges
+    and gives the complex128 observables."""
+    from bdda_b200.inputs import so3_euler
+    from bdda_b200.shapes import gre_particle
+    from bl_dda import scatterer as sc
+    wl, mp = 0.85, 1.53 + 0.005j
+    g = gre_particle(4.403823395619191, 0.7398419617561375, 0.7475936957677011, 0.029412861486646926, 3002,
+                     wl_0=1.0, m_m=1.0, workers=1)
+    sc.DiscreteDipoles.verbose = False
+    out = {}
+    for prec in (None, "mixed"):
+        t = sc.Target("gre2", g["lattice_n"], g["lattice_lf"] * wl, g["grid"] * wl, g["is_in"], [mp] * 3)
+        d = sc.DiscreteDipoles(t, sc.IncidentField(wl, 1.0, so3_euler(32, 308)))
+        d.tol, d.itermax, d.precision = 1e-5, 500, prec
+        d.set_interaction_matrix()
+        d.solve_matrix_equation()
+        assert d.converge and d.err_fin < 1e-5, (prec, d.iter_fin, d.err_fin)
+        out[prec] = (d.iter_fin, d.observables())
+    assert out["mixed"][0] <= 120
+    o64, om = out[None][1], out["mixed"][1]
+    for cols in ((1,), (2, 3), (4, 5), (10, 11)):
+        a = om[:, cols[0]] + (1j * om[:, cols[1]] if len(cols) > 1 else 0)
+        b = o64[:, cols[0]] + (1j * o64[:, cols[1]] if len(cols) > 1 else 0)
+        assert np.max(np.abs(a - b)) / np.max(np.abs(b)) < 1e-3, cols
 
 
 def test_mixed_form_converges_where_fp32_krylov_diverges(mods):
