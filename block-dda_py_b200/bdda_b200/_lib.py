@@ -34,6 +34,9 @@ _pd = C.POINTER(C.c_double)
 # tests check the two lists against each other.
 PROTOTYPES = {
     "bdda_status_string": (C.c_char_p, [_i]),
+    "bdda_gre_occupancy_workspace_bytes": (_sz, [_i, _i, _i]),
+    "bdda_gre_occupancy": (_i, [_i, _i, _i, _vp, _vp, _vp, _i, _vp, _vp, _i, _i, _i, _d, _d, _d, _d, _d, _vp, _vp,
+                                _vp, _sz, _vp]),
     "bdda_version": (_i, []),
     "bdda_tune_set": (_i, [_i, _i, _sz, _i]),
     "bdda_tune_get": (_i, [_i, _i, C.POINTER(_sz), _pi]),

@@ -74,14 +74,78 @@ def inside_mask(near: np.ndarray) -> np.ndarray:
     return inside
 
 
+def reference_spacing(r_v_base: float, bc: float, ab: float) -> tuple[float, float]:
+    """Default lattice spacing and near-surface distance factor of the reference's
+    shape model for these axes (gaussian_ellipsoid.py:64-70)."""
+    c = np.cbrt(r_v_base ** 3 / (ab * bc ** 2))
+    lf = (1 / 75) * np.sqrt(c / 0.05) * (ab * bc) ** (1 / 5)
+    dfac = 3 ** 0.5 / 2 * (bc * ab * (c / 0.1)) ** (1 / 6)
+    return float(lf), float(dfac)
+
+
+def gre_name(r_v_base: float, ab: float, bc: float, beta: float) -> str:
+    """The reference's shape name string (gaussian_ellipsoid.py:86-89)."""
+    return ("GRE_shape__r_v_base={:.2f}um__ab_ratio={:.1f}"
+            "__bc_ratio={:.1f}__beta={:.2f}".format(r_v_base, ab, bc, beta))
+
+
+def lattice_axes(surf: np.ndarray, lf: float) -> list[np.ndarray]:
+    """Cell centres per axis of the cuboid enclosing the surface (gaussian_ellipsoid.py:150-180)."""
+    lim = np.max(np.abs(surf), axis=0) + lf
+    return [np.arange(-lim[i], lim[i], lf) for i in range(3)]
+
+
+def gre_geometry(r_v_base: float, bc: float, ab: float, beta: float, seed: int, lattice_lf: float | None = None,
+                 mask_fn=None, workers: int = -1) -> dict:
+    """The reference's geometry pipeline for one shape (run_dda.py:21-35).
+
+    Same arguments and defaults as ``gaussian_ellipsoid_shape_model(r_v_base,
+    bc_ratio, ab_ratio, beta)`` followed by the surface draw from
+    ``default_rng(seed)``, the enclosing lattice, the nearest-surface distance
+    and the three-axis inside test.  ``lattice_lf`` overrides the default
+    spacing.  ``mask_fn(axes, surf, thr) -> inside (Nx, Ny, Nz) bool`` decides
+    the occupied cells (default: a k-d tree and cumulative sums on the host;
+    :func:`bdda_b200.geometry.inside_from_gpu` runs both on the GPU).  Returns
+    ``name, lattice_n, lattice_lf, x_axis, y_axis, z_axis, is_in, address,
+    grid, r_ve``.
+    """
+    lf0, dfac = reference_spacing(r_v_base, bc, ab)
+    lf = lf0 if lattice_lf is None else float(lattice_lf)
+    rng = np.random.default_rng(seed)
+    surf = gre_surface(r_v_base, ab, bc, beta, rng)
+    axes = lattice_axes(surf, lf)
+    n = np.array([len(v) for v in axes], dtype=np.int64)
+    thr = dfac * lf
+    if mask_fn is None:
+        is_in = inside_mask(host_near_surface(axes, surf, thr, workers)).ravel()
+    else:
+        is_in = np.asarray(mask_fn(axes, surf, thr), dtype=bool).ravel()
+    X, Y, Z = np.meshgrid(*axes, indexing="ij")
+    grid = np.column_stack([X.ravel(), Y.ravel(), Z.ravel()])
+    n_in = int(is_in.sum())
+    return dict(name=gre_name(r_v_base, ab, bc, beta), lattice_n=n, lattice_lf=lf, x_axis=axes[0],
+                y_axis=axes[1], z_axis=axes[2], is_in=is_in, address=np.flatnonzero(is_in), grid=grid,
+                r_ve=float(np.cbrt(3.0 * lf ** 3 * n_in / (4 * np.pi))))
+
+
+def host_near_surface(axes, surf: np.ndarray, thr: float, workers: int = -1) -> np.ndarray:
+    """Cells whose centre lies closer than ``thr`` to a surface point (k-d tree, host)."""
+    X, Y, Z = np.meshgrid(*axes, indexing="ij")
+    grid = np.column_stack([X.ravel(), Y.ravel(), Z.ravel()])
+    dist, _ = scipy.spatial.cKDTree(surf).query(grid, k=1, distance_upper_bound=thr, workers=workers)
+    return (dist < thr).reshape(tuple(len(v) for v in axes))
+
+
 def gre_particle(x: float, ab: float, bc: float, beta: float, seed: int, wl_0: float = 1.0, m_m: float = 1.0,
-                 ppl: float = 16.0, coarse: tuple[int, int] = (25, 100), workers: int = -1) -> dict:
+                 ppl: float = 16.0, coarse: tuple[int, int] = (25, 100), workers: int = -1,
+                 mask_fn=None) -> dict:
     """GRE of size parameter x = 2 pi r_v / lambda_m on a lattice of spacing lambda_m / ppl.
 
     Returns a geometry record like :func:`bdda_b200.inputs.load_geometry`:
     ``lattice_n``, ``lattice_lf``, the axis arrays, ``is_in``, ``address``,
     ``grid`` (cell centres) plus the shape parameters.  ``workers``: threads
-    of the nearest-surface query (-1: all cores).
+    of the nearest-surface query (-1: all cores); ``mask_fn`` as for
+    :func:`gre_geometry` (the GPU decides the occupied cells).
     """
     lam = wl_0 / m_m
     r_v = x * lam / (2.0 * np.pi)
@@ -96,9 +160,11 @@ def gre_particle(x: float, ab: float, bc: float, beta: float, seed: int, wl_0: f
     a, b, c = gre_axes(r_v, ab, bc)
     dfac = np.sqrt(3.0) / 2.0 * (bc * ab * (c / 0.1)) ** (1.0 / 6.0)
     thr = dfac * lf
-    dist, _ = scipy.spatial.cKDTree(surf).query(grid, k=1, distance_upper_bound=thr, workers=workers)
-    near = (dist < thr).reshape(tuple(n))
-    is_in = inside_mask(near).ravel()
+    if mask_fn is None:
+        dist, _ = scipy.spatial.cKDTree(surf).query(grid, k=1, distance_upper_bound=thr, workers=workers)
+        is_in = inside_mask((dist < thr).reshape(tuple(n))).ravel()
+    else:
+        is_in = np.asarray(mask_fn(axes, surf, thr), dtype=bool).ravel()
     return dict(lattice_n=n, lattice_lf=float(lf), x_axis=axes[0], y_axis=axes[1], z_axis=axes[2],
                 is_in=is_in, address=np.flatnonzero(is_in), grid=grid, wl_0=float(wl_0), m_m=float(m_m),
                 x=float(x), ab=float(ab), bc=float(bc), beta=float(beta), seed=int(seed))

@@ -262,7 +262,8 @@ def bl_bicgstab_jacobi_mvp_fft_batch(problems, tol, itermax, precision=None, max
     solver.  ``precision``: "c128" (default), "c64", or "mixed" (complex128
     Krylov vectors with complex64 products, judged on the complex128 true
     residual, at most ``max_outer`` warm-restarted rounds; problems it leaves
-    above ``tol`` are solved again in complex128, iter_fin counting both).
+    above ``tol`` are solved again in complex128 from their start, with the
+    iterations they have left, iter_fin counting both).
     ``graph``
     replays the batched iteration as a CUDA graph.  ``history`` (list)
     receives one residual list per problem, ``statuses`` (list) one status
@@ -347,14 +348,17 @@ def bl_bicgstab_jacobi_mvp_fft_batch(problems, tol, itermax, precision=None, max
     if mode == _lib.BATCH_MIXED:
         # problems the mixed form leaves above tol (its recursion diverged under the
         # complex64 products) are solved again with complex128 products
-        redo = [i for i, r in enumerate(results) if r[3] == 1 and not r[2] < tol]
-        if redo:
+        # with the iterations the batch left them (iter_fin counts both), so no
+        # problem takes more than itermax iterations in all
+        redo = [i for i, r in enumerate(results) if r[3] == 1 and not r[2] < tol and itermax - 1 - r[1] > 0]
+        for left in sorted({itermax - 1 - results[i][1] for i in redo}):
+            sub = [i for i in redo if itermax - 1 - results[i][1] == left]
             sub_hist = [] if history is not None else None
             sub_st = []
-            again = bl_bicgstab_jacobi_mvp_fft_batch([problems[i] for i in redo], tol, itermax, "c128",
+            again = bl_bicgstab_jacobi_mvp_fft_batch([problems[i] for i in sub], tol, left, "c128",
                                                      max_outer, graph, sub_hist, sub_st,
                                                      max_bytes if fixed_bound else None)
-            for j, i in enumerate(redo):
+            for j, i in enumerate(sub):
                 X, it, er = again[j]
                 results[i] = (X, results[i][1] + 1 + it, er, sub_st[j])
                 if history is not None:

@@ -18,7 +18,10 @@
 //    zero, because each product writes every scratch element before reading it;
 //  - the first call on a device looks up the array's device address with that
 //    device current (cudaGetSymbolAddress); make that first call before any
-//    stream capture.
+//    stream capture.  The address is kept for the life of the process, so
+//    cudaDeviceReset on a device that has called this entry point is not
+//    supported (the reset unloads the array; a later call would use a stale
+//    address).
 #include <mutex>
 
 #include "bdda_internal.h"

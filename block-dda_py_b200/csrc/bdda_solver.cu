@@ -377,13 +377,16 @@ static int bicgstab_core(Ctx<T>& c, bool has_x0, double tol, int itermax, int* i
       BDDA_CUDA_TRY(cudaGetLastError());
       TRY(read_state(c, &err, &bad));
       rmax = err;
+      // keep X for a warm fallback when its true residual is the smallest so
+      // far (one copy per replacement, not per iteration)
+      if (c.xbest && bad == 0 && err < c.best) {
+        BDDA_CUDA_TRY(cudaMemcpyAsync(c.xbest, X, (size_t)c.n * L * sizeof(T), cudaMemcpyDeviceToDevice,
+                                      c.stream));
+        c.best = err;
+      }
       if (err < g_mixed_switch * tol) c.ghat32 = nullptr;   // complex128 products from here on
     }
     rmax = err > rmax ? err : rmax;
-    if (c.xbest && c.ghat32 && bad == 0 && err < c.best) {   // keep X for a warm fallback
-      BDDA_CUDA_TRY(cudaMemcpyAsync(c.xbest, X, (size_t)c.n * L * sizeof(T), cudaMemcpyDeviceToDevice, c.stream));
-      c.best = err;
-    }
     rmin = err < rmin ? err : rmin;
     if (hist) hist[k] = err;
     *iter_fin = k;
@@ -837,8 +840,8 @@ static int run_refine(int solver, bool restart, const bdda_plan* p, int L, int n
 // not below tol the solver restarts from the current X (warm start).  A
 // BiCGSTAB recursion that diverges under the complex64 products is abandoned
 // and the problem solved on with complex128 products, warm-started from the X
-// of the smallest residual the recursion reached (kept in xbest) when that
-// is below the zero start's.
+// of the smallest true residual seen at a replacement (kept in xbest) when
+// that is below the zero start's.
 constexpr double kInnerFrac = 0.5;
 
 struct MLayout {

@@ -28,6 +28,7 @@
  *  bl_krylov/bl_krylov.py:121 bl_bicgstab_jacobi_mvp_fft -> bdda_bicgstab
  *  bl_dda/scatterer.py:135-161 set_interaction_matrix (diag_A, B) -> bdda_polarizability, bdda_incident_rhs
  *  bl_dda/scatterer.py:182-227 E, C_abs, C_ext, S_fw, S_bk       -> bdda_observables
+ *  shape_model/gaussian_ellipsoid.py:182-237 near-surface distance + inside test -> bdda_gre_occupancy
  */
 #ifndef BDDA_H
 #define BDDA_H
@@ -164,7 +165,8 @@ int bdda_block_mvp(const bdda_plan* plan, int prec, int L, const void* ghat,
  * share the array: calls that overlap on the GPU race, so serialise them.
  * Nothing in it needs to start at zero.  The first call on a device looks up
  * the array's address with that device current; make it before any stream
- * capture.  It allocates nothing (cudaMalloc, cudaFree and allocating library
+ * capture.  That address is kept until exit: do not cudaDeviceReset a device
+ * after calling this entry point on it.  It allocates nothing (cudaMalloc, cudaFree and allocating library
  * routines are never called; profiling, off by default, creates CUDA events). */
 size_t bdda_block_mvp_noalloc_max_bytes(void);
 int bdda_block_mvp_noalloc_fits(const bdda_plan* plan, int prec, int L);
@@ -387,6 +389,25 @@ int bdda_observables(int n_occ, int L, double k, double lf, int absorbing, const
 unsigned long long bdda_launch_count(void);
 int bdda_profile_enable(int on);
 int bdda_profile_read(int prec, double pass_ms[5], long long* n_mvp);
+
+/* ---- GRE lattice occupancy (shape_model/gaussian_ellipsoid.py:182-237) -------
+ * replaces find_nearest_distance_from_the_GRE_surf (:182-192, a k-d tree
+ * query) and extract_lattice_address_in_GRE_volume (:195-237).  Cell (i,j,k)
+ * of the nx x ny x nz lattice sits at (xs[i], ys[j], zs[k]) (the reference's
+ * axis arrays); near[c] = 1 when some surface point lies closer than thr
+ * (distance evaluated as the reference, sqrt((dx^2 + dy^2) + dz^2), each
+ * operation rounded); inside[c] = 1 when near cells lie strictly before and
+ * strictly after c along all three axes.  c = (i ny + j) nz + k.  The npts
+ * surface points (x, y, z doubles) must be sorted by bin of a uniform grid
+ * of nbx x nby x nbz bins of edge h >= thr whose corner is (ox, oy, oz):
+ * bin b = (bx nby + by) nbz + bz, bx = floor((x - ox) / h); points of bin b
+ * are pts[bin_start[b] .. bin_start[b+1]).  All arrays are device memory;
+ * work holds bdda_gre_occupancy_workspace_bytes(). */
+size_t bdda_gre_occupancy_workspace_bytes(int nx, int ny, int nz);
+int bdda_gre_occupancy(int nx, int ny, int nz, const double* xs, const double* ys, const double* zs, int npts,
+                       const double* pts, const int32_t* bin_start, int nbx, int nby, int nbz, double ox,
+                       double oy, double oz, double h, double thr, uint8_t* near, uint8_t* inside, void* work,
+                       size_t work_bytes, void* stream);
 
 #ifdef __cplusplus
 }

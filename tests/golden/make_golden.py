@@ -1,9 +1,13 @@
 """Generate the golden fixtures in this folder from the live reference.
 
-Run in a container where the reference block-DDA_Py v0.3.0 is checked out
-(default ``/root/reference``, override with ``BDDA_REFERENCE``):
+Run in a container where the reference block-DDA_Py v0.3.0 is checked out,
+naming its folder with ``--reference`` or the ``BDDA_REFERENCE`` variable:
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py --reference PATH [fixture ...]
+
+With no fixture names the small fixtures are written; ``solve_cfg2_chunk``
+(minutes of CPU and ~14 GB of RAM), ``sweep_small`` and ``mie_small`` are
+written when named.
 
 The reference is imported as-is; ``matplotlib`` (absent in this image, used
 only for plotting in shape_model/gaussian_ellipsoid.py:4-8,41) is replaced by
@@ -22,20 +26,29 @@ kat_test_dda.npz     inputs and reference outputs of test_dda.ipynb
 geometry_cfg1.npz    sphere x=5, wl=1, m_m=1, spacing 1/16 -> 28^3 lattice,
                      plus the reference's COCG-rq solution to 1e-5 at L=8
 geometry_cfg2.npz    GRE x=20 (m_m=1.33, wl=1), ab 0.7, bc 0.8, beta 0.1,
-                     surface seed 1, spacing lambda_m/16 -> 96x111x160
+                     surface seed 1, spacing lambda_m/16 -> 93x112x174
+solve_cfg2_chunk.npz the reference's block-BiCGSTAB solve of that particle,
+                     orientations 0-7 of the seed-2 set, to 1e-5: iteration
+                     count, residual history, observables, sampled rows of X
+sweep_small.npz      a 2 x 2 x 2-shape sweep run as run_dda.py runs it (shape
+                     seed 12345, angle seed 12346, retries, Mie values), in
+                     the reference's 7-D layout
+mie_small.npz        the reference's Mie routine on six spheres
 """
 from __future__ import annotations
 
+import argparse
 import contextlib
 import io
 import os
 import sys
+import time
 import types
 
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = os.environ.get("BDDA_REFERENCE", "/root/reference")
+REF = os.environ.get("BDDA_REFERENCE")
 
 
 def _stub_matplotlib() -> None:
@@ -54,6 +67,9 @@ def _stub_matplotlib() -> None:
 
 
 def _import_reference():
+    if not REF or not os.path.isdir(os.path.join(REF, "bl_krylov")):
+        raise SystemExit("make_golden: pass --reference PATH (or set BDDA_REFERENCE) to the "
+                         "block-DDA_Py checkout; got %r" % (REF,))
     _stub_matplotlib()
     sys.path.insert(0, REF)
     from mvp_fft import mvp_fft
@@ -132,8 +148,44 @@ def run_reference_solve(sc, bk, geo, m_p_xyz, wl_0, m_m, euler, solver, tol, ite
                 diag_A=dd.diag_A, B=dd.B, ve_radius=dd.ve_radius, dpl=dd.dpl)
 
 
-def main() -> None:
-    mf, bk, sc, ge = _import_reference()
+CFG2_M_P = np.array([1.55 + 0.001j, 1.60 + 0.001j, 1.52 + 0.002j])
+
+
+def cfg2_geometry(ge):
+    """Config 2 particle: GRE x=20 (m_m=1.33, wl=1), ab 0.7, bc 0.8, beta 0.1, seed 1, lambda_m/16."""
+    m_m, wl_0 = 1.33, 1.0
+    lam_m = wl_0 / m_m
+    r_v = 20.0 * lam_m / (2 * np.pi)
+    return gre_geometry(ge, r_v, 0.8, 0.7, 0.1, 1, lattice_lf=lam_m / 16), wl_0, m_m
+
+
+def cfg2_chunk_fixture(bk, sc, ge) -> dict:
+    """The reference's own block-BiCGSTAB solve of config 2, orientations 0-7, to 1e-5.
+
+    The solve runs through the reference's DiscreteDipoles + bl_bicgstab_jacobi_mvp_fft
+    on all host threads (DDA_FFT_WORKERS as set by the caller); its wall time is
+    recorded beside the results.  X (168 MB) is kept only at 96 evenly spaced
+    dipoles.
+    """
+    geo, wl_0, m_m = cfg2_geometry(ge)
+    euler = so3_euler(64, 2)[:8]
+    t0 = time.perf_counter()
+    res = run_reference_solve(sc, bk, geo, CFG2_M_P, wl_0, m_m, euler, "bicgstab", 1e-5, 300)
+    wall = time.perf_counter() - t0
+    n_occ = int(geo["is_in"].sum())
+    dip = np.unique(np.linspace(0, n_occ - 1, 96).astype(np.int64))
+    rows = (3 * dip[:, None] + np.arange(3)[None, :]).ravel()
+    from mvp_fft import mvp_fft as _mf
+    rec = dict(lattice_n=geo["lattice_n"], n_occ=n_occ, mask_bits=np.packbits(geo["is_in"]),
+               euler=euler, m_p_xyz=CFG2_M_P, wl_0=wl_0, m_m=m_m, tol=1e-5, itermax=300,
+               sample_dipoles=dip, X_rows=res["X"][rows],
+               wall_s=wall, cpu_count=os.cpu_count() or 1, fft_workers=int(_mf._FFT_WORKERS))
+    rec.update({k2: res[k2] for k2 in ("iter_fin", "err_fin", "history", "C_abs", "C_ext",
+                                       "S_fw_theta", "S_fw_phi", "S_bk")})
+    return rec
+
+
+def small_fixtures(mf, bk, sc, ge) -> dict:
     rng = np.random.default_rng(20261203)
     out = {}
 
@@ -227,16 +279,127 @@ def main() -> None:
             rec[tag + key] = r[key]
     out["geometry_cfg1"] = rec
 
-    # --- config 2 geometry only (the solve is GPU-scale) ---------------------------
-    m_m, wl_0 = 1.33, 1.0
-    lam_m = wl_0 / m_m
-    r_v = 20.0 * lam_m / (2 * np.pi)
-    geo = gre_geometry(ge, r_v, 0.8, 0.7, 0.1, 1, lattice_lf=lam_m / 16)
+    # --- config 2 geometry --------------------------------------------------------
+    geo, wl_0, m_m = cfg2_geometry(ge)
     rec = geometry_record(geo)
-    rec.update(euler=so3_euler(64, 2), wl_0=wl_0, m_m=m_m,
-               m_p_xyz=np.array([1.55 + 0.001j, 1.60 + 0.001j, 1.52 + 0.002j]))
+    rec.update(euler=so3_euler(64, 2), wl_0=wl_0, m_m=m_m, m_p_xyz=CFG2_M_P)
     out["geometry_cfg2"] = rec
+    return out
 
+
+SWEEP_SMALL = dict(wl_m_m_pairs=np.array([[0.633, 1.330], [0.8337, 1.329]]),
+                   m_p_xyz_list=np.array([[1.5 + 0j] * 3, [1.55 + 0.01j, 1.5 + 0.01j, 1.6 + 0.02j]]),
+                   r_v_base_list=np.array([0.08, 0.12]), bc_ratio_list=np.array([1.5]),
+                   ab_ratio_list=np.array([1.2]), gre_beta_list=np.array([0.1]), num_orientations=8,
+                   rng_seed=12345, max_try=4)
+
+
+def sweep_small_fixture(sc, ge, mie) -> dict:
+    """A small sweep run the way run_dda.py runs one (run_dda.py:21-146), with the
+    reference's own classes; run_dda.py itself opens an HDF5 file at import
+    time, so its loop is restated here step for step."""
+    sp = SWEEP_SMALL
+    P, M = len(sp["wl_m_m_pairs"]), len(sp["m_p_xyz_list"])
+    geo_shape = (len(sp["r_v_base_list"]), len(sp["bc_ratio_list"]), len(sp["ab_ratio_list"]),
+                 len(sp["gre_beta_list"]))
+    L = sp["num_orientations"]
+    cond = (P, M) + geo_shape
+    out = {k: v for k, v in sp.items()}
+    out["r_ve"] = np.zeros(geo_shape)
+    out["Euler_angles"] = np.zeros(cond + (L, 3))
+    for k in ("C_abs", "C_ext"):
+        out[k] = np.zeros(cond + (L,))
+    for k in ("S_fw_PCAS_theta", "S_fw_PCAS_phi", "S_bk_OCBS"):
+        out[k] = np.zeros(cond + (L,), dtype=np.complex128)
+    for k in ("C_abs_mie", "C_ext_mie"):
+        out[k] = np.zeros(cond)
+    for k in ("S_fw_PCAS_mie", "S_bk_OCBS_mie"):
+        out[k] = np.zeros(cond, dtype=np.complex128)
+    out["tries"] = np.zeros(cond, dtype=np.int64)
+    for i_rv, rv in enumerate(sp["r_v_base_list"]):
+        for i_bc, bc in enumerate(sp["bc_ratio_list"]):
+            for i_ab, ab in enumerate(sp["ab_ratio_list"]):
+                for i_bt, bt in enumerate(sp["gre_beta_list"]):
+                    s4 = (i_rv, i_bc, i_ab, i_bt)
+                    rng = np.random.default_rng(sp["rng_seed"])
+                    gre = ge.gaussian_ellipsoid_shape_model(rv, bc, ab, bt)
+                    r_pts, _ = gre.compute_r_points_on_GRE(rng)
+                    _, lattice_n, grid = gre.create_cuboid_lattice_that_encloses_GRE_shape(r_pts)
+                    dist = gre.find_nearest_distance_from_the_GRE_surf(grid, r_pts)
+                    is_in = gre.extract_lattice_address_in_GRE_volume(gre.lattice_lf, gre.distance_factor,
+                                                                      lattice_n, dist)
+                    r_ve = np.cbrt(3.0 * gre.lattice_lf ** 3 * int(is_in.sum()) / (4 * np.pi))
+                    out["r_ve"][s4] = r_ve
+                    for i_pair, (wl_0, m_m) in enumerate(sp["wl_m_m_pairs"]):
+                        for i_mp, m_p_xyz in enumerate(sp["m_p_xyz_list"]):
+                            idx6 = (i_pair, i_mp) + s4
+                            target = sc.Target(gre.name, lattice_n, gre.lattice_lf, grid, is_in, m_p_xyz)
+                            rng2 = np.random.default_rng(sp["rng_seed"] + 1)
+                            res = None
+                            for i_try in range(1, sp["max_try"] + 1):
+                                euler = np.column_stack([rng2.uniform(0, 2 * np.pi, L), rng2.uniform(0, np.pi, L),
+                                                         rng2.uniform(0, 2 * np.pi, L)])
+                                with contextlib.redirect_stdout(io.StringIO()):
+                                    dd = sc.DiscreteDipoles(target, sc.IncidentField(wl_0, m_m, euler))
+                                    dd.set_interaction_matrix()
+                                    dd.solve_matrix_equation()
+                                if dd.converge:
+                                    res = (dd.compute_C_abs(), dd.compute_C_ext(),
+                                           *dd.compute_PCAS_observable_S_fw(), dd.compute_OCBS_observable_S_bk())
+                                    break
+                            if res is None:
+                                res = tuple(np.full(L, np.nan) for _ in range(5))
+                            out["Euler_angles"][idx6] = euler
+                            out["tries"][idx6] = i_try
+                            for k, v in zip(("C_abs", "C_ext", "S_fw_PCAS_theta", "S_fw_PCAS_phi", "S_bk_OCBS"),
+                                            res):
+                                out[k][idx6] = v
+                            _, q_abs, q_ext, s_fw, s_bk = mie.mie_compute_q_and_s(
+                                wl_0, m_m, r_ve, complex(np.mean(m_p_xyz)), nang=3)
+                            out["C_abs_mie"][idx6] = q_abs * np.pi * r_ve ** 2
+                            out["C_ext_mie"][idx6] = q_ext * np.pi * r_ve ** 2
+                            out["S_fw_PCAS_mie"][idx6] = s_fw
+                            out["S_bk_OCBS_mie"][idx6] = s_bk
+    return out
+
+
+def mie_fixture(mie) -> dict:
+    """The reference's Mie routine on a spread of sizes and indices (complex64 amplitudes)."""
+    cases = [(0.633, 1.33, 0.05, 1.5 + 0j), (0.8337, 1.329, 0.2027, 1.5 + 0.05j), (0.55, 1.0, 0.5, 1.53 + 0.005j),
+             (1.0, 1.0, 5 / (2 * np.pi), 1.5 + 0.01j), (0.45, 1.0, 1.2, 1.6 + 0.1j), (0.532, 1.331, 0.01, 2.0 + 1.0j)]
+    rows = np.array([[wl, mm, r, mp.real, mp.imag] for wl, mm, r, mp in cases])
+    q = np.array([mie.mie_compute_q_and_s(wl, mm, r, mp, nang=3)[:3] for wl, mm, r, mp in cases])
+    s = np.array([mie.mie_compute_q_and_s(wl, mm, r, mp, nang=3)[3:] for wl, mm, r, mp in cases])
+    return dict(cases=rows, Q_sca_abs_ext=q, S_fw_bk=s.astype(np.complex128))
+
+
+SMALL = ("green_small", "fft_mvp_small", "block_mvp_small", "solver_small", "kat_test_dda",
+         "geometry_cfg1", "geometry_cfg2")
+
+
+def main(argv=None) -> None:
+    global REF
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--reference", default=None, help="block-DDA_Py checkout (else $BDDA_REFERENCE)")
+    ap.add_argument("fixtures", nargs="*", help="fixture names (default: all small ones)")
+    a = ap.parse_args(argv)
+    REF = a.reference or REF
+    names = a.fixtures or list(SMALL)
+    unknown = set(names) - set(SMALL) - {"solve_cfg2_chunk", "sweep_small", "mie_small"}
+    if unknown:
+        raise SystemExit("unknown fixture(s): %s" % sorted(unknown))
+    mf, bk, sc, ge = _import_reference()
+    out = {}
+    if set(names) & set(SMALL):
+        out.update({k: v for k, v in small_fixtures(mf, bk, sc, ge).items() if k in names})
+    if "sweep_small" in names or "mie_small" in names:
+        from analytical_scattering_theories import homogeneous_sphere as mie
+        if "sweep_small" in names:
+            out["sweep_small"] = sweep_small_fixture(sc, ge, mie)
+        if "mie_small" in names:
+            out["mie_small"] = mie_fixture(mie)
+    if "solve_cfg2_chunk" in names:
+        out["solve_cfg2_chunk"] = cfg2_chunk_fixture(bk, sc, ge)
     for name, rec in out.items():
         path = os.path.join(HERE, name + ".npz")
         np.savez_compressed(path, **rec)

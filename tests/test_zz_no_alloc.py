@@ -42,10 +42,17 @@ def test_noalloc_block_mvp_matches_workspace_entry_point():
         out = torch.empty_like(S)
         _lib.check(lib.bdda_block_mvp(plan.handle, _lib.C128, L, ptr(gh), ptr(occ.cell_map), ptr(diag),
                                       ptr(jpre), ptr(S), ptr(ref), ptr(work), stream_ptr()), "bdda_block_mvp")
+        torch.cuda.synchronize()
+        free_before = torch.cuda.mem_get_info()[0]
         _lib.check(lib.bdda_block_mvp_noalloc(plan.handle, _lib.C128, L, ptr(gh), ptr(occ.cell_map), ptr(diag),
                                               ptr(jpre), ptr(S), ptr(out), stream_ptr()),
                    "bdda_block_mvp_noalloc")
         torch.cuda.synchronize()
+        free_after = torch.cuda.mem_get_info()[0]
+        if call == 1:
+            # the first call may load the library's device code (and with it the
+            # static array); from then on a call takes no device memory at all
+            assert free_after == free_before, (free_before, free_after)
         err = (out - ref).abs().max().item() / ref.abs().max().item()
         assert err < TOL, (call, err)
 
