@@ -40,6 +40,13 @@ sys.path.insert(0, REPO)
 GEOMETRY = os.path.join(REPO, "tests", "golden", "geometry_cfg2.npz")
 METRIC = "orientations/s to rel-res 1e-5: plain FP64 vs FP32+refine+NN warm start, 1 B200"
 TOL = 1e-5
+# Stopping tolerance of the headline runs.  At the metric's 1e-5 the
+# rounding-level drift between two solves (even two complex128 solves; the
+# reference itself moves S_bk by ~1e-5 under a 1e-16 change of B) leaves S_bk
+# of the mixed form ~3e-4 from the FP64 path's; at this tolerance both paths'
+# observables agree within the 1e-4 gate.  Both forms at 1e-5 are reported
+# beside it (at_metric_tol).
+TOL_GATE = 2e-6
 ITERMAX = 500
 # DRAM bytes (read + write) of the five complex64 passes (Z, Y, X, Y^-1, Z^-1) of this
 # workload's product at L = 8, from one ncu capture of `bench.py --mvp-only --L 8`
@@ -50,11 +57,11 @@ DRAM_L8_C64 = (0.7316e9, 2.0403e9, 3.4710e9, 2.0569e9, 0.8936e9)
 DRAM_L8_CONST = (0.0072e9, 0.0, 0.7225e9, 0.0, 0.0072e9)
 
 
-def workload_config(L):
+def workload_config(L, tol=TOL):
     return {"workload": "GRE x=20 ab0.7 bc0.8 beta0.1 seed1, m_m 1.33, lambda_m/16 -> 93x112x174 lattice, "
-                        "438606 dipoles, L=%d SO(3) orientations (seed 2), block-BiCGSTAB to 1e-5" % L,
+                        "438606 dipoles, L=%d SO(3) orientations (seed 2), block-BiCGSTAB to %g" % (L, tol),
             "lattice": [93, 112, 174], "n_dipoles": 438606, "orientations": L, "solver": "block-BiCGSTAB",
-            "tol": TOL, "l2": "inputs larger than L2 (working set ~35 GB >> 126 MB)"}
+            "tol": tol, "l2": "inputs larger than L2 (working set ~35 GB >> 126 MB)"}
 
 
 def load_workload(L):
@@ -149,10 +156,12 @@ def run_bdda(args, rank, world, local_rank):
     geo, euler = load_workload(L)
     mixed = args.form == "mixed"
 
-    def make_dd(precision):
+    tol = args.tol
+
+    def make_dd(precision, tol_=None):
         t = sc.Target("gre", geo["lattice_n"], geo["lattice_lf"], geo["grid"], geo["is_in"], geo["m_p_xyz"])
         dd = sc.DiscreteDipoles(t, sc.IncidentField(float(geo["wl_0"]), float(geo["m_m"]), euler))
-        dd.tol, dd.itermax = TOL, ITERMAX
+        dd.tol, dd.itermax = (tol if tol_ is None else tol_), ITERMAX
         dd.precision = precision
         return dd
 
@@ -214,31 +223,54 @@ def run_bdda(args, rank, world, local_rank):
     clocks = clk.summary()
     iters = dd.iter_fin + 1
 
-    # ---- the plain FP64 path beside it (the metric's comparison) ----
+    # ---- the plain FP64 path beside it (the metric's comparison), the accuracy
+    # gate, and both forms at the metric's own tolerance ----
+    def rel_errs(o, r):
+        out = {}
+        for name, cols in (("C_ext", (1,)), ("S_fw_theta", (2, 3)), ("S_fw_phi", (4, 5)), ("S_bk", (10, 11))):
+            a = o[:, cols[0]] + (1j * o[:, cols[1]] if len(cols) > 1 else 0)
+            b = r[:, cols[0]] + (1j * r[:, cols[1]] if len(cols) > 1 else 0)
+            out[name] = float("%.3g" % (np.max(np.abs(a - b)) / np.max(np.abs(b))))
+        return out
+
     plain = None
+    accuracy = None
+    metric_tol = None
     if mixed and not args.no_fp64:
         d64 = make_dd(None)
         device_step(d64)
         ms64, obs64 = timed(d64, args.steps)
         # converged FP64 solution (tol 1e-10), untimed: the accuracy reference
-        dref = make_dd(None)
-        dref.tol, dref.itermax = 1e-10, 400
+        dref = make_dd(None, 1e-10)
+        dref.itermax = 400
         obsref = device_step(dref)
-
-        def rel_errs(o, r):
-            out = {}
-            for name, cols in (("C_ext", (1,)), ("S_fw_theta", (2, 3)), ("S_fw_phi", (4, 5)),
-                               ("S_bk", (10, 11))):
-                a = o[:, cols[0]] + (1j * o[:, cols[1]] if len(cols) > 1 else 0)
-                b = r[:, cols[0]] + (1j * r[:, cols[1]] if len(cols) > 1 else 0)
-                out[name] = float("%.3g" % (np.max(np.abs(a - b)) / np.max(np.abs(b))))
-            return out
-        plain = {"value": round(world * L / (ms64 * 1e-3), 3), "unit": "orientations/s",
+        err_mv64 = rel_errs(obs, obs64)
+        plain = {"value": round(world * L / (ms64 * 1e-3), 3), "unit": "orientations/s", "tol": tol,
                  "ms_per_step": round(ms64, 3), "iterations": d64.iter_fin + 1,
-                 "speedup_of_mixed": round(ms64 / ms, 3),
-                 "max_rel_err_mixed_vs_fp64": rel_errs(obs, obs64),
-                 "max_rel_err_vs_converged_fp64": {"mixed": rel_errs(obs, obsref),
-                                                   "fp64_tol1e-5": rel_errs(obs64, obsref)}}
+                 "speedup_of_mixed": round(ms64 / ms, 3)}
+        accuracy = {"gate": "max rel. error of C_ext, S_fw (theta, phi), S_bk, mixed vs FP64 at the same "
+                            "tolerance, <= 1e-4", "tol": tol,
+                    "max_rel_err_mixed_vs_fp64": err_mv64,
+                    "accuracy_ok": bool(max(err_mv64.values()) <= 1e-4),
+                    "max_rel_err_vs_converged_fp64": {"mixed": rel_errs(obs, obsref),
+                                                      "fp64": rel_errs(obs64, obsref)}}
+        if tol != TOL:   # both forms at the metric's tolerance too, labelled
+            ksteps = max(2, args.steps // 4)
+            dm5, d645 = make_dd("mixed", TOL), make_dd(None, TOL)
+            device_step(dm5)
+            ms_m5, obs_m5 = timed(dm5, ksteps)
+            device_step(d645)
+            ms_645, obs_645 = timed(d645, ksteps)
+            e5 = rel_errs(obs_m5, obs_645)
+            metric_tol = {"tol": TOL, "steps": ksteps,
+                          "mixed": {"value": round(world * L / (ms_m5 * 1e-3), 3), "ms_per_step": round(ms_m5, 3),
+                                    "iterations": dm5.iter_fin + 1},
+                          "fp64": {"value": round(world * L / (ms_645 * 1e-3), 3), "ms_per_step": round(ms_645, 3),
+                                   "iterations": d645.iter_fin + 1},
+                          "speedup_of_mixed": round(ms_645 / ms_m5, 3),
+                          "max_rel_err_mixed_vs_fp64": e5, "accuracy_ok": bool(max(e5.values()) <= 1e-4),
+                          "max_rel_err_vs_converged_fp64": {"mixed": rel_errs(obs_m5, obsref),
+                                                            "fp64": rel_errs(obs_645, obsref)}}
 
     # ---- end to end through the public API, host numpy in and out ----
     def e2e_step():
@@ -302,12 +334,19 @@ def run_bdda(args, rank, world, local_rank):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "complex64 products, complex128 Krylov + true residual" if mixed else "complex128",
         "form": args.form,
+        "tol": tol,
         "data": "synthetic: reference GRE geometry (seed 1) and SO(3) orientations (seed 2)",
-        "config": dict(workload_config(L), parallelism="replicas x%d" % world,
+        "config": dict(workload_config(L, tol), parallelism="replicas x%d" % world,
                        green_build_s=round(green_s, 4), autotune_s=round(tune_s, 2),
                        autotune_mvp_ms={k: [round(v[0], 3), round(v[1], 3)] for k, v in tuned.items()}, iterations=iters, converged=dd.converge,
-                       true_residual=dd.err_fin if mixed else None),
+                       true_residual=dd.err_fin if mixed else None, tol=tol,
+                       tol_note=None if tol == TOL else
+                       "stopping tolerance %g, stricter than the metric's %g, so that the mixed form's "
+                       "observables stay within 1e-4 of the FP64 path's (accuracy gate); both forms at %g "
+                       "are in at_metric_tol" % (tol, TOL, TOL)),
         "plain_fp64": plain,
+        "accuracy": accuracy,
+        "at_metric_tol": metric_tol,
         "e2e": {"value": round(world * L / e2e_s, 3), "unit": "orientations/s",
                 "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                 "includes": "Target/IncidentField/DiscreteDipoles from host arrays, Green build, solve, "
@@ -717,6 +756,8 @@ def main():
     ap.add_argument("--form", default="mixed", choices=["mixed", "fp64", "fp32"],
                     help="mixed: FP32 block solves inside FP64 refinement (headline); fp64: plain complex128")
     ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 comparison run")
+    ap.add_argument("--tol", type=float, default=TOL_GATE,
+                    help="stopping tolerance of the timed solves (default: the accuracy-gate tolerance)")
     ap.add_argument("--L", type=int, default=64)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--mvp-only", action="store_true", help="time block MVPs of the workload only")

@@ -35,6 +35,9 @@ _pd = C.POINTER(C.c_double)
 PROTOTYPES = {
     "bdda_status_string": (C.c_char_p, [_i]),
     "bdda_gre_occupancy_workspace_bytes": (_sz, [_i, _i, _i]),
+    "bdda_dda_workspace_bytes": (_sz, [_vp, _i, _i, _i]),
+    "bdda_dda_solve": (_i, [_vp, _vp, _i, _i, _vp, _vp, _vp, _vp, _d, _i, _i, _vp, _vp, _vp, _vp, _pi, _pd, _pd,
+                            _vp, _sz, _vp]),
     "bdda_gre_occupancy": (_i, [_i, _i, _i, _vp, _vp, _vp, _i, _vp, _vp, _i, _i, _i, _d, _d, _d, _d, _d, _vp, _vp,
                                 _vp, _sz, _vp]),
     "bdda_version": (_i, []),

@@ -21,6 +21,13 @@ from bl_krylov import bl_krylov
 from mvp_fft.mvp_fft import fft_init
 
 
+class _DdaProblem(C.Structure):
+    """include/bdda.h: bdda_dda_problem."""
+    _fields_ = [("n_occ", C.c_int), ("L", C.c_int), ("m_p_xyz", C.c_double * 6), ("m_m", C.c_double),
+                ("lf", C.c_double), ("k", C.c_double), ("absorbing", C.c_int), ("pos", C.c_void_p),
+                ("vec", C.c_void_p), ("e0", C.c_void_p)]
+
+
 def _rot_z(t):
     c, s = np.cos(t), np.sin(t)
     R = np.zeros(t.shape + (3, 3))
@@ -141,20 +148,15 @@ class DiscreteDipoles(Target, IncidentField):
         return self._dev["vec"]
 
     def set_interaction_matrix(self, m=None, green=None):
-        """Diagonal (CR2009 polarizability), Green's spectrum and RHS on the GPU (scatterer.py:135-161).
+        """Green's spectrum, and the diagonal and right-hand side on the GPU (scatterer.py:135-161).
 
         ``green`` (optional) is a spectrum from ``fft_init`` for the same
         lattice, spacing and wavenumber, reused instead of being rebuilt.
+        diag_A and B are formed by the solve itself (``bdda_dda_solve``
+        builds M^-1 B from the positions in its prologue and never stores B);
+        reading ``diag_A`` or ``B`` before, or solving through another entry
+        point, materialises them with the polarizability and RHS kernels.
         """
-        lib = _lib.load()
-        N, L = self.num_element_occupy, self.L
-        pos = self._geometry_to_device()
-        mp = np.asarray(self.m_p_xyz).astype(np.complex128)
-        mpd = (C.c_double * 6)(*[float(v) for z in mp for v in (z.real, z.imag)])
-        diag = torch.empty(3 * N, dtype=torch.complex128, device=self.device)
-        eper = torch.empty(3 * N, dtype=torch.complex128, device=self.device)
-        _lib.check(lib.bdda_polarizability(N, mpd, float(self.m_m), float(self.lattice_lf), float(self.k),
-                                           ptr(diag), ptr(eper), stream_ptr(self.device)), "bdda_polarizability")
         if green is not None:
             if (green.plan.n != tuple(int(v) for v in self.lattice_n) or green.lf != float(self.lattice_lf)
                     or green.k != float(self.k)):
@@ -164,30 +166,129 @@ class DiscreteDipoles(Target, IncidentField):
             self.Au_til = fft_init(self.lattice_n, self.f, self.lattice_lf, self.k, m=m)
         if self._dev.get("occ") is None or self._dev["occ"].plan is not self.Au_til.plan:
             self._dev["occ"] = Occupancy(self.Au_til.plan, self.lattice_address_in_target)
+        self._geometry_to_device()
         self._geometry_vectors()
-        B = torch.empty((3 * N, L), dtype=torch.complex128, device=self.device)
-        _lib.check(lib.bdda_incident_rhs(N, L, float(self.k), ptr(pos), ptr(self._dev["u_inc"]),
-                                         ptr(self._dev["e0"]), ptr(B), stream_ptr(self.device)),
-                   "bdda_incident_rhs")
-        self._dev.update(diag=diag, eper=eper, B=B)
-        self._dev.pop("X", None)
+        for key in ("diag", "eper", "B", "X", "obs"):
+            self._dev.pop(key, None)
         self._host.clear()
         self._obs = None
 
+    def _m_p_doubles(self):
+        mp = np.asarray(self.m_p_xyz).astype(np.complex128)
+        return [float(v) for z in mp for v in (z.real, z.imag)]
+
+    def _materialize(self):
+        """diag_A, eps_r and B as device arrays (polarizability and RHS kernels)."""
+        if "diag" in self._dev and "B" in self._dev:
+            return
+        if self.Au_til is None:
+            raise ValueError("call set_interaction_matrix() first")
+        lib = _lib.load()
+        N, L = self.num_element_occupy, self.L
+        if "diag" not in self._dev or "eper" not in self._dev:
+            diag = torch.empty(3 * N, dtype=torch.complex128, device=self.device)
+            eper = torch.empty(3 * N, dtype=torch.complex128, device=self.device)
+            mpd = (C.c_double * 6)(*self._m_p_doubles())
+            _lib.check(lib.bdda_polarizability(N, mpd, float(self.m_m), float(self.lattice_lf), float(self.k),
+                                               ptr(diag), ptr(eper), stream_ptr(self.device)),
+                       "bdda_polarizability")
+            self._dev.update(diag=diag, eper=eper)
+        B = torch.empty((3 * N, L), dtype=torch.complex128, device=self.device)
+        _lib.check(lib.bdda_incident_rhs(N, L, float(self.k), ptr(self._geometry_to_device()),
+                                         ptr(self._dev["u_inc"]), ptr(self._dev["e0"]), ptr(B),
+                                         stream_ptr(self.device)), "bdda_incident_rhs")
+        self._dev["B"] = B
+
+    def _fused_solve(self, X0, solver, mode):
+        """set-up + solve + observables in one library call per block of <= 64 orientations."""
+        lib = _lib.load()
+        N, L = self.num_element_occupy, self.L
+        g = self.Au_til
+        plan = g.plan
+        occ = self._dev["occ"]
+        dev = self.device
+        need64 = mode != _lib.BATCH_C64
+        need32 = mode != _lib.BATCH_C128
+        diag = torch.empty(3 * N, dtype=torch.complex128, device=dev)
+        eper = torch.empty(3 * N, dtype=torch.complex128, device=dev)
+        X = torch.empty((3 * N, L), dtype=torch.complex128, device=dev)
+        obs = torch.empty((L, 12), dtype=torch.float64, device=dev)
+        X0d = None if X0 is None else to_device(X0, torch.complex128, dev).reshape(3 * N, L)
+        nblk = (L + 63) // 64
+        bounds = [(b * L // nblk, (b + 1) * L // nblk) for b in range(nblk)]
+        iters, errs = [], []
+        vec, e0 = self._dev["vec"], self._dev["e0"]
+        itermax = int(self.itermax)
+        for l0, l1 in bounds:
+            Lb = l1 - l0
+            prob = _DdaProblem()
+            prob.n_occ, prob.L = N, Lb
+            prob.m_p_xyz = (C.c_double * 6)(*self._m_p_doubles())
+            prob.m_m, prob.lf, prob.k = float(self.m_m), float(self.lattice_lf), float(self.k)
+            prob.absorbing = self._absorbing()
+            prob.pos = ptr(self._geometry_to_device())
+            vb = vec[l0:l1].contiguous()
+            eb = e0[l0:l1].contiguous()
+            prob.vec, prob.e0 = ptr(vb), ptr(eb)
+            Xb = X if nblk == 1 else torch.empty((3 * N, Lb), dtype=torch.complex128, device=dev)
+            ob = obs if nblk == 1 else torch.empty((Lb, 12), dtype=torch.float64, device=dev)
+            X0b = None if X0d is None else (X0d if nblk == 1 else X0d[:, l0:l1].contiguous())
+            nbytes = int(lib.bdda_dda_workspace_bytes(plan.handle, mode, Lb, N))
+            work = torch.empty(max(nbytes, 16), dtype=torch.uint8, device=dev)
+            hist = (C.c_double * max(itermax, 1))()
+            it = C.c_int(0)
+            err = C.c_double(float("inf"))
+            status = lib.bdda_dda_solve(plan.handle, C.byref(prob), solver, mode,
+                                        ptr(g.ghat(_lib.C128)) if need64 else None,
+                                        ptr(g.ghat(_lib.C64)) if need32 else None, ptr(occ.cell_map), ptr(X0b),
+                                        float(self.tol), itermax, 20, ptr(Xb), ptr(diag), ptr(eper), ptr(ob),
+                                        C.byref(it), C.byref(err), hist, ptr(work), nbytes, stream_ptr(dev))
+            if status == _lib.BREAKDOWN:
+                raise np.linalg.LinAlgError("Singular matrix")
+            _lib.check(status, "bdda_dda_solve")
+            del work
+            if nblk > 1:
+                X[:, l0:l1] = Xb
+                obs[l0:l1] = ob
+            iters.append(it.value)
+            errs.append(err.value)
+        self._dev.update(diag=diag, eper=eper, X=X, obs=obs)
+        # one block: the solver's own values; several: the largest (a bound on the
+        # residual of the whole block, whose columns were solved in groups of <= 64)
+        return max(iters), max(errs)
+
     def solve_matrix_equation(self, X0=None, solver=None, precision=None):
-        """Block solve to ``self.tol`` within ``self.itermax`` (scatterer.py:164-184)."""
+        """Block solve to ``self.tol`` within ``self.itermax`` (scatterer.py:164-184).
+
+        The complex128 (default), complex64 and "mixed" forms run the fused
+        entry point bdda_dda_solve: right-hand side, solve and observables in
+        one call.  Other ``precision`` forms go through ``bl_krylov``.  More
+        than 64 orientations are solved in blocks of at most 64.
+        """
         solver = solver or self.solver
         precision = precision if precision is not None else self.precision
         start = time.time()
         if self.verbose:
             print("Starting block-%s iterative solver..." % ("BiCGStab" if solver == "bicgstab" else "COCG-rq"))
-        fn = (bl_krylov.bl_cocg_rq_jacobi_mvp_fft if solver == "cocg"
-              else bl_krylov.bl_bicgstab_jacobi_mvp_fft)
-        X, iter_fin, err_fin = fn(self.lattice_n, self.f, self._dev["occ"], self.Au_til,
-                                  self._dev["diag"], self._dev["B"], self.tol, self.itermax, X0=X0,
-                                  precision=precision)
+        if self.Au_til is None:
+            raise ValueError("call set_interaction_matrix() first")
+        key = "c128" if precision is None else str(precision).lower()
+        modes = {"c128": _lib.BATCH_C128, "fp64": _lib.BATCH_C128, "complex128": _lib.BATCH_C128,
+                 "c64": _lib.BATCH_C64, "fp32": _lib.BATCH_C64, "complex64": _lib.BATCH_C64,
+                 "mixed": _lib.BATCH_MIXED}
+        kind = _lib.COCG_RQ if solver == "cocg" else _lib.BICGSTAB
+        if key in modes:
+            iter_fin, err_fin = self._fused_solve(X0, kind, modes[key])
+        else:
+            self._materialize()
+            fn = (bl_krylov.bl_cocg_rq_jacobi_mvp_fft if solver == "cocg"
+                  else bl_krylov.bl_bicgstab_jacobi_mvp_fft)
+            X, iter_fin, err_fin = fn(self.lattice_n, self.f, self._dev["occ"], self.Au_til,
+                                      self._dev["diag"], self._dev["B"], self.tol, self.itermax, X0=X0,
+                                      precision=precision)
+            self._dev["X"] = X
+            self._dev.pop("obs", None)
         self.iter_fin, self.err_fin = iter_fin, err_fin
-        self._dev["X"] = X
         self._host.pop("X", None)
         self._obs = None
         elapsed = time.time() - start
@@ -202,13 +303,18 @@ class DiscreteDipoles(Target, IncidentField):
             self._host[key] = fn()
         return self._host[key]
 
+    def _dev_array(self, key):
+        if key not in self._dev:
+            self._materialize()
+        return self._dev[key]
+
     @property
     def eper_r(self):
-        return self._np("eper_r", lambda: self._dev["eper"].cpu().numpy().reshape(-1, 3))
+        return self._np("eper_r", lambda: self._dev_array("eper").cpu().numpy().reshape(-1, 3))
 
     @property
     def diag_A(self):
-        return self._np("diag_A", lambda: self._dev["diag"].cpu().numpy())
+        return self._np("diag_A", lambda: self._dev_array("diag").cpu().numpy())
 
     @property
     def alpha_E(self):
@@ -216,7 +322,7 @@ class DiscreteDipoles(Target, IncidentField):
 
     @property
     def B(self):
-        return self._np("B", lambda: self._dev["B"].cpu().numpy())
+        return self._np("B", lambda: self._dev_array("B").cpu().numpy())
 
     @property
     def E_inc(self):
@@ -251,6 +357,8 @@ class DiscreteDipoles(Target, IncidentField):
         Computed in one pass on the GPU from the solution.  Like the
         reference, a solve that did not converge leaves P = E = 0.
         """
+        if self._obs is None and "obs" in self._dev:   # from the fused solve (zeros if not converged)
+            self._obs = self._dev["obs"].cpu().numpy()
         if self._obs is None:
             lib = _lib.load()
             N, L = self.num_element_occupy, self.L
@@ -261,7 +369,7 @@ class DiscreteDipoles(Target, IncidentField):
             work = torch.empty(max(int(lib.bdda_observables_workspace_bytes(L)), 16), dtype=torch.uint8,
                                device=self.device)
             _lib.check(lib.bdda_observables(N, L, float(self.k), float(self.lattice_lf), self._absorbing(),
-                                            ptr(self._geometry_to_device()), ptr(self._dev["eper"]), ptr(X),
+                                            ptr(self._geometry_to_device()), ptr(self._dev_array("eper")), ptr(X),
                                             ptr(self._geometry_vectors()), ptr(self._dev["e0"]), ptr(out),
                                             ptr(work), stream_ptr(self.device)), "bdda_observables")
             self._obs = out.cpu().numpy()
@@ -317,6 +425,7 @@ def solve_matrix_equations(dds, X0s=None, precision=None, graph=True):
     for i, d in enumerate(dds):
         if d.Au_til is None:
             raise ValueError("call set_interaction_matrix() first")
+        d._materialize()
         p = (d.lattice_n, d._dev["occ"], d.Au_til, d._dev["diag"], d._dev["B"])
         x0 = None if X0s is None else X0s[i]
         probs.append(p if x0 is None else p + (x0,))
@@ -326,6 +435,7 @@ def solve_matrix_equations(dds, X0s=None, precision=None, graph=True):
     for d, (X, it, err) in zip(dds, res):
         d.iter_fin, d.err_fin = it, err
         d._dev["X"] = X
+        d._dev.pop("obs", None)
         d._host.pop("X", None)
         d._obs = None
         d.converge = bool(err < d.tol)

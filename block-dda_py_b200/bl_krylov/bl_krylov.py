@@ -82,7 +82,8 @@ def _solve(kind, n, f, address, Au_til, DIAG_A, B, tol, itermax, X0=None, precis
         raise ValueError("B must be (%d, L), got %r" % (3 * occ.n_occ, tuple(Bd.shape)))
     L = int(Bd.shape[1])
     if L > 64:
-        raise ValueError("at most 64 right-hand sides per block solve (got L=%d); split the block" % L)
+        return _solve_in_blocks(kind, n, f, occ, g, DIAG_A, Bd, tol, itermax, X0, precision, history, verbose,
+                                inner_tol, max_outer, to_numpy)
     diag = to_device(DIAG_A, torch.complex128, plan.device).reshape(-1)
     if diag.numel() != 3 * occ.n_occ:
         raise ValueError("DIAG_A must have %d entries" % (3 * occ.n_occ))
@@ -127,6 +128,35 @@ def _solve(kind, n, f, address, Au_til, DIAG_A, B, tol, itermax, X0=None, precis
             print("iter= {:}, err= {:.4f}".format(i, hist[i]))
     del work
     return (X.cpu().numpy() if to_numpy else X), it.value, err.value
+
+
+def _solve_in_blocks(kind, n, f, occ, g, DIAG_A, Bd, tol, itermax, X0, precision, history, verbose, inner_tol,
+                     max_outer, to_numpy):
+    """More than 64 right-hand sides: ceil(L / 64) column blocks of near-equal
+    width solved one after another (the reference iterates on all L columns as
+    one block).  iter_fin and err_fin are the largest of the blocks' (the
+    largest relative residual bounds that of the whole block); ``history``
+    receives, per iteration, the largest residual among the blocks still
+    iterating."""
+    L = int(Bd.shape[1])
+    nblk = (L + 63) // 64
+    X = torch.empty_like(Bd)
+    X0d = None if X0 is None else to_device(X0, torch.complex128, Bd.device).reshape(Bd.shape)
+    its, errs, hists = [], [], []
+    for b in range(nblk):
+        l0, l1 = b * L // nblk, (b + 1) * L // nblk
+        h = []
+        Xb, it, err = _solve(kind, n, f, occ, g, DIAG_A, Bd[:, l0:l1].contiguous(), tol, itermax,
+                             None if X0d is None else X0d[:, l0:l1].contiguous(), precision, h, verbose,
+                             inner_tol, max_outer)
+        X[:, l0:l1] = Xb
+        its.append(it)
+        errs.append(err)
+        hists.append(h)
+    if history is not None:
+        for k in range(max(len(h) for h in hists)):
+            history.append(max(h[k] for h in hists if k < len(h)))
+    return (X.cpu().numpy() if to_numpy else X), max(its), max(errs)
 
 
 def bl_cocg_rq_jacobi_mvp_fft(n, f, address, Au_til, DIAG_A, B, tol, itermax, X0=None,

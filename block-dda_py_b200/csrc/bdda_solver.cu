@@ -14,6 +14,7 @@
 #include "bdda_internal.h"
 #include "bdda_small.cuh"
 #include "bdda_steps.cuh"
+#include "bdda_dda.cuh"
 
 namespace bdda {
 
@@ -231,6 +232,7 @@ struct Ctx {
   bool diverged = false;   // set when the complex64-product recursion blew up
   T* xbest = nullptr;      // mixed form: X at the smallest residual so far (or null)
   double best = INFINITY;  // that residual
+  bool replaced = false;   // a residual replacement has happened
   bool watch = false;      // apply the divergence test to complex128 products too
 };
 
@@ -377,14 +379,21 @@ static int bicgstab_core(Ctx<T>& c, bool has_x0, double tol, int itermax, int* i
       BDDA_CUDA_TRY(cudaGetLastError());
       TRY(read_state(c, &err, &bad));
       rmax = err;
-      // keep X for a warm fallback when its true residual is the smallest so
-      // far (one copy per replacement, not per iteration)
+      // keep X for a warm fallback when its true residual is the smallest so far
       if (c.xbest && bad == 0 && err < c.best) {
         BDDA_CUDA_TRY(cudaMemcpyAsync(c.xbest, X, (size_t)c.n * L * sizeof(T), cudaMemcpyDeviceToDevice,
                                       c.stream));
         c.best = err;
       }
+      c.replaced = true;
       if (err < g_mixed_switch * tol) c.ghat32 = nullptr;   // complex128 products from here on
+    }
+    // before the first replacement, X is kept at every new minimum of the
+    // recursive residual (a divergence can come first); after it, only at
+    // replacements, so the copies do not run every iteration
+    if (c.xbest && c.ghat32 && !c.replaced && bad == 0 && err < c.best) {
+      BDDA_CUDA_TRY(cudaMemcpyAsync(c.xbest, X, (size_t)c.n * L * sizeof(T), cudaMemcpyDeviceToDevice, c.stream));
+      c.best = err;
     }
     rmax = err > rmax ? err : rmax;
     rmin = err < rmin ? err : rmin;
@@ -493,11 +502,35 @@ static int allow_smem(K kern, size_t bytes) {
   return BDDA_OK;
 }
 
+// Epilogue of the fused entry point: X widened into Xout and the observables
+// accumulated in the same pass; a solve that did not converge reports zero
+// observables (P = E = 0).
+template <typename T>
+static int dda_epilogue(const DdaPhys& ph, const T* X, double2* Xout, bool converged, cudaStream_t st) {
+  const int L = ph.L;
+  dda_epilogue_kernel<T><<<kDdaObsBlocks, dda_epilogue_threads(L), dda_epilogue_smem(L), st>>>(ph, X, Xout,
+                                                                                               nullptr);
+  BDDA_CUDA_TRY(cudaGetLastError());
+  count_launch();
+  if (converged) {
+    observables_finalize_kernel<<<(L + 63) / 64, 64, 0, st>>>(ph.partial, kDdaObsBlocks, L, ph.k, ph.absorbing,
+                                                               ph.obs);
+    BDDA_CUDA_TRY(cudaGetLastError());
+    count_launch();
+  } else {
+    BDDA_CUDA_TRY(cudaMemsetAsync(ph.obs, 0, (size_t)L * 12 * sizeof(double), st));
+  }
+  return BDDA_OK;
+}
+
+// phys (nullable): the fused DDA entry point; the right-hand side and diagonal
+// come from the physics (diag and B unused) and the epilogue adds the observables.
 template <typename T>
 static int run_solver(int solver, const bdda_plan* p, int L, int n_occ, const void* ghat,
                       const int32_t* cell_map, const double2* diag, const double2* B, const double2* X0,
                       double tol, int itermax, double2* Xout, int* iter_fin, double* err_fin,
-                      double* hist, void* work, size_t work_bytes, cudaStream_t st) {
+                      double* hist, void* work, size_t work_bytes, cudaStream_t st,
+                      const DdaPhys* phys = nullptr) {
   const int prec = std::is_same<T, double2>::value ? BDDA_C128 : BDDA_C64;
   const Layout o = layout(p, prec, L, n_occ);
   if (work_bytes < o.total) return BDDA_NO_WORKSPACE;
@@ -527,7 +560,11 @@ static int run_solver(int solver, const bdda_plan* p, int L, int n_occ, const vo
   BDDA_CUDA_TRY(cudaMemsetAsync(c.st, 0, sizeof(SolverState), st));
   constants_kernel<<<1, 32, 0, st>>>(c.sp);
   count_launch();
-  prepare_kernel<T><<<kRedBlocks, 256, 0, st>>>(diag, B, c.n, L, c.diag, c.jpre, c.vec[7]);
+  if (phys) {
+    dda_prologue_kernel<T, false><<<kRedBlocks, 256, 0, st>>>(*phys, c.diag, c.jpre, c.vec[7], nullptr, nullptr);
+  } else {
+    prepare_kernel<T><<<kRedBlocks, 256, 0, st>>>(diag, B, c.n, L, c.diag, c.jpre, c.vec[7]);
+  }
   count_launch();
   BDDA_CUDA_TRY(cudaGetLastError());
   if (X0) {
@@ -541,9 +578,13 @@ static int run_solver(int solver, const bdda_plan* p, int L, int n_occ, const vo
                          ? cocg_core<T>(c, X0 != nullptr, tol, itermax, iter_fin, err_fin, hist)
                          : bicgstab_core<T>(c, X0 != nullptr, tol, itermax, iter_fin, err_fin, hist);
   if (status == BDDA_OK || status == BDDA_NOT_CONVERGED) {
-    convert_out_kernel<T><<<kRedBlocks, 256, 0, st>>>(c.vec[0], Xout, c.n * L);
-    count_launch();
-    BDDA_CUDA_TRY(cudaGetLastError());
+    if (phys) {
+      TRY(dda_epilogue<T>(*phys, c.vec[0], Xout, status == BDDA_OK, st));
+    } else {
+      convert_out_kernel<T><<<kRedBlocks, 256, 0, st>>>(c.vec[0], Xout, c.n * L);
+      count_launch();
+      BDDA_CUDA_TRY(cudaGetLastError());
+    }
   }
   return status;
 }
@@ -840,8 +881,9 @@ static int run_refine(int solver, bool restart, const bdda_plan* p, int L, int n
 // not below tol the solver restarts from the current X (warm start).  A
 // BiCGSTAB recursion that diverges under the complex64 products is abandoned
 // and the problem solved on with complex128 products, warm-started from the X
-// of the smallest true residual seen at a replacement (kept in xbest) when
-// that is below the zero start's.
+// of the smallest residual (kept in xbest: at each new minimum until the first
+// residual replacement, then at replacements) when that is below the zero
+// start's.
 constexpr double kInnerFrac = 0.5;
 
 struct MLayout {
@@ -866,7 +908,7 @@ static MLayout mlayout(const bdda_plan* p, int L, int n_occ) {
 static int run_mixed(int solver, const bdda_plan* p, int L, int n_occ, const void* ghat64, const void* ghat32,
                      const int32_t* cell_map, const double2* diag, const double2* B, const double2* X0, double tol,
                      int itermax, int max_outer, double2* Xout, int* iter_fin, double* err_fin, double* hist,
-                     void* work, size_t work_bytes, cudaStream_t st) {
+                     void* work, size_t work_bytes, cudaStream_t st, const DdaPhys* phys = nullptr) {
   const MLayout o = mlayout(p, L, n_occ);
   if (work_bytes < o.total) return BDDA_NO_WORKSPACE;
   unsigned char* w = static_cast<unsigned char*>(work);
@@ -889,9 +931,14 @@ static int run_mixed(int solver, const bdda_plan* p, int L, int n_occ, const voi
   if (solver == BDDA_BICGSTAB) c.xbest = reinterpret_cast<double2*>(w + o.xbest);
   BDDA_CUDA_TRY(cudaMemsetAsync(c.st, 0, sizeof(SolverState), st));
   constants_kernel<<<1, 32, 0, st>>>(c.sp);
-  prepare_kernel<double2><<<kRedBlocks, 256, 0, st>>>(diag, B, c.n, L, c.diag, c.jpre, Bj);
-  prepare_kernel<float2><<<kRedBlocks, 256, 0, st>>>(diag, B, c.n, L, diag32, jpre32, in32);
-  count_launch(3);
+  if (phys) {
+    dda_prologue_kernel<double2, true><<<kRedBlocks, 256, 0, st>>>(*phys, c.diag, c.jpre, Bj, diag32, jpre32);
+    count_launch(2);
+  } else {
+    prepare_kernel<double2><<<kRedBlocks, 256, 0, st>>>(diag, B, c.n, L, c.diag, c.jpre, Bj);
+    prepare_kernel<float2><<<kRedBlocks, 256, 0, st>>>(diag, B, c.n, L, diag32, jpre32, in32);
+    count_launch(3);
+  }
   BDDA_CUDA_TRY(cudaGetLastError());
   if (X0) BDDA_CUDA_TRY(cudaMemcpyAsync(X, X0, (size_t)ne * sizeof(double2), cudaMemcpyDeviceToDevice, st));
   else BDDA_CUDA_TRY(cudaMemsetAsync(X, 0, (size_t)ne * sizeof(double2), st));
@@ -970,7 +1017,11 @@ static int run_mixed(int solver, const bdda_plan* p, int L, int n_occ, const voi
     if (!(err < 0.9 * prev)) break;   // restarts no longer gain
     prev = err;
   }
-  BDDA_CUDA_TRY(cudaMemcpyAsync(Xout, X, (size_t)ne * sizeof(double2), cudaMemcpyDeviceToDevice, st));
+  if (phys) {
+    TRY(dda_epilogue<double2>(*phys, X, Xout, status == BDDA_OK, st));
+  } else {
+    BDDA_CUDA_TRY(cudaMemcpyAsync(Xout, X, (size_t)ne * sizeof(double2), cudaMemcpyDeviceToDevice, st));
+  }
   return status;
 }
 
@@ -1098,6 +1149,74 @@ int bdda_mixed_solve(const bdda_plan* p, int solver, int L, int n_occ, const voi
                    static_cast<const double2*>(B), static_cast<const double2*>(X0), tol, itermax, max_outer,
                    static_cast<double2*>(X), iter_fin, err_fin, history, work, work_bytes,
                    static_cast<cudaStream_t>(stream));
+}
+
+size_t bdda_dda_workspace_bytes(const bdda_plan* p, int mode, int L, int n_occ) {
+  if (!p || L < 1 || L > kMaxL || n_occ < 1) return 0;
+  size_t base;
+  if (mode == BDDA_BATCH_MIXED) base = mlayout(p, L, n_occ).total;
+  else if (mode == BDDA_BATCH_C128 || mode == BDDA_BATCH_C64) base = layout(p, mode, L, n_occ).total;
+  else return 0;
+  return al(base) + al((size_t)kDdaObsBlocks * L * 10 * sizeof(double));
+}
+
+int bdda_dda_solve(const bdda_plan* p, const bdda_dda_problem* prob, int solver, int mode, const void* ghat_c128,
+                   const void* ghat_c64, const int32_t* cell_map, const void* X0, double tol, int itermax,
+                   int max_outer, void* X, void* diag_out, void* eper_out, double* obs, int* iter_fin,
+                   double* err_fin, double* history, void* work, size_t work_bytes, void* stream) {
+  if (!p || !prob || prob->L < 1 || prob->L > kMaxL || prob->n_occ < 1 || !prob->pos || !prob->vec || !prob->e0 ||
+      !(prob->lf > 0.0) || !(prob->m_m > 0.0) || !cell_map || !X || !obs || !iter_fin || !err_fin ||
+      itermax < 0 || !(tol == tol) || (solver != BDDA_BICGSTAB && solver != BDDA_COCG_RQ))
+    return BDDA_BAD_ARG;
+  if (mode != BDDA_BATCH_C128 && mode != BDDA_BATCH_C64 && mode != BDDA_BATCH_MIXED) return BDDA_BAD_ARG;
+  if ((mode != BDDA_BATCH_C64 && !ghat_c128) || (mode != BDDA_BATCH_C128 && !ghat_c64)) return BDDA_BAD_ARG;
+  if (mode == BDDA_BATCH_MIXED && (max_outer < 1 || !(tol > 0.0))) return BDDA_BAD_ARG;
+  const int L = prob->L, n_occ = prob->n_occ;
+  const size_t need = bdda_dda_workspace_bytes(p, mode, L, n_occ);
+  if (!work || !p->dev_tables || work_bytes < need) return BDDA_NO_WORKSPACE;
+  const size_t base = need - al((size_t)kDdaObsBlocks * L * 10 * sizeof(double));
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  DdaPhys ph;
+  memset(&ph, 0, sizeof(ph));
+  ph.n_occ = n_occ; ph.L = L;
+  for (int c = 0; c < 3; ++c) ph.mp[c] = make_double2(prob->m_p_xyz[2 * c], prob->m_p_xyz[2 * c + 1]);
+  ph.m_m = prob->m_m; ph.lf = prob->lf; ph.k = prob->k; ph.absorbing = prob->absorbing;
+  ph.pos = prob->pos; ph.vec = prob->vec; ph.e0 = static_cast<const double2*>(prob->e0);
+  ph.diag_out = static_cast<double2*>(diag_out);
+  ph.eper_out = static_cast<double2*>(eper_out);
+  ph.obs = obs;
+  ph.partial = reinterpret_cast<double*>(static_cast<unsigned char*>(work) + base);
+  *iter_fin = 0;
+  *err_fin = INFINITY;
+  double2* Xd = static_cast<double2*>(X);
+  const double2* X0d = static_cast<const double2*>(X0);
+  if (itermax == 0) {   // the reference returns X = 0 without iterating; the set-up outputs are still made
+    unsigned char* w = static_cast<unsigned char*>(work);
+    if (mode == BDDA_BATCH_C64) {
+      const Layout o = layout(p, BDDA_C64, L, n_occ);
+      dda_prologue_kernel<float2, false><<<kRedBlocks, 256, 0, st>>>(
+          ph, reinterpret_cast<float2*>(w + o.diag), reinterpret_cast<float2*>(w + o.jpre),
+          reinterpret_cast<float2*>(w + o.vec[7]), nullptr, nullptr);
+    } else {   // the complex128 layout (also the base of the mixed one)
+      const Layout o = layout(p, BDDA_C128, L, n_occ);
+      dda_prologue_kernel<double2, false><<<kRedBlocks, 256, 0, st>>>(
+          ph, reinterpret_cast<double2*>(w + o.diag), reinterpret_cast<double2*>(w + o.jpre),
+          reinterpret_cast<double2*>(w + o.vec[7]), nullptr, nullptr);
+    }
+    count_launch();
+    BDDA_CUDA_TRY(cudaGetLastError());
+    BDDA_CUDA_TRY(cudaMemsetAsync(X, 0, (size_t)3 * n_occ * L * sizeof(double2), st));
+    BDDA_CUDA_TRY(cudaMemsetAsync(obs, 0, (size_t)L * 12 * sizeof(double), st));
+    return BDDA_NOT_CONVERGED;
+  }
+  if (mode == BDDA_BATCH_MIXED)
+    return run_mixed(solver, p, L, n_occ, ghat_c128, ghat_c64, cell_map, nullptr, nullptr, X0d, tol, itermax,
+                     max_outer, Xd, iter_fin, err_fin, history, work, base, st, &ph);
+  if (mode == BDDA_BATCH_C128)
+    return run_solver<double2>(solver, p, L, n_occ, ghat_c128, cell_map, nullptr, nullptr, X0d, tol, itermax, Xd,
+                               iter_fin, err_fin, history, work, base, st, &ph);
+  return run_solver<float2>(solver, p, L, n_occ, ghat_c64, cell_map, nullptr, nullptr, X0d, tol, itermax, Xd,
+                            iter_fin, err_fin, history, work, base, st, &ph);
 }
 
 }  // extern "C"

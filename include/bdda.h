@@ -28,6 +28,7 @@
  *  bl_krylov/bl_krylov.py:121 bl_bicgstab_jacobi_mvp_fft -> bdda_bicgstab
  *  bl_dda/scatterer.py:135-161 set_interaction_matrix (diag_A, B) -> bdda_polarizability, bdda_incident_rhs
  *  bl_dda/scatterer.py:182-227 E, C_abs, C_ext, S_fw, S_bk       -> bdda_observables
+ *  bl_dda/scatterer.py:135-227 set_interaction_matrix + solve_matrix_equation + compute_* -> bdda_dda_solve
  *  shape_model/gaussian_ellipsoid.py:182-237 near-surface distance + inside test -> bdda_gre_occupancy
  */
 #ifndef BDDA_H
@@ -389,6 +390,42 @@ int bdda_observables(int n_occ, int L, double k, double lf, int absorbing, const
 unsigned long long bdda_launch_count(void);
 int bdda_profile_enable(int on);
 int bdda_profile_read(int prec, double pass_ms[5], long long* n_mvp);
+
+/* ---- one DDA solve: set-up, block solve and observables in one call --------
+ * replaces, for one particle and L orientations, set_interaction_matrix
+ * (bl_dda/scatterer.py:135-161; the Green's spectrum ghat comes from
+ * bdda_green_build), solve_matrix_equation (:164-184, block-BiCGSTAB as the
+ * reference or block-COCG-rq) and compute_C_abs / compute_C_ext /
+ * compute_PCAS_observable_S_fw / compute_OCBS_observable_S_bk (:187-227).
+ * The prologue forms diag_A and the Jacobi-scaled right-hand side M^-1 B
+ * directly from the positions and incident vectors (B is never stored); the
+ * epilogue accumulates the observables in the pass that writes X.
+ * mode: BDDA_BATCH_C128 (ghat_c128), BDDA_BATCH_C64 (ghat_c64) or
+ * BDDA_BATCH_MIXED (both; max_outer warm-restarted rounds, as
+ * bdda_mixed_solve).  Outputs: X (3N, L) c128; obs (L, 12) doubles on the
+ * device = C_abs, C_ext, S_fw_theta (re, im), S_fw_phi (re, im), S_bk_theta
+ * (re, im), S_bk_phi (re, im), S_bk (re, im), all zero when the solve did
+ * not converge (the reference sets P = E only on convergence); diag_out and
+ * eper_out (3N c128, nullable) receive diag_A and eps_r.  Return codes and
+ * iter_fin / err_fin / history as bdda_solve (bdda_mixed_solve in the mixed
+ * mode). */
+typedef struct bdda_dda_problem {
+  int n_occ;            /* occupied dipoles N */
+  int L;                /* orientations (<= 64) */
+  double m_p_xyz[6];    /* particle index per axis: re, im of x, y, z */
+  double m_m;           /* medium index */
+  double lf;            /* lattice spacing */
+  double k;             /* wavenumber in the medium, 2 pi m_m / wl_0 */
+  int absorbing;        /* 1: C_abs computed (mean Im eps_r >= 1e-12, scatterer.py:189); 0: C_abs = 0 */
+  const double* pos;    /* (N, 3) dipole positions, device */
+  const double* vec;    /* (L, 21) per orientation: u_inc, u_fw, theta_fw, phi_fw, u_bk, theta_bk, phi_bk */
+  const void* e0;       /* (L, 3) c128 incident polarisation vectors, device */
+} bdda_dda_problem;
+size_t bdda_dda_workspace_bytes(const bdda_plan* plan, int mode, int L, int n_occ);
+int bdda_dda_solve(const bdda_plan* plan, const bdda_dda_problem* prob, int solver, int mode, const void* ghat_c128,
+                   const void* ghat_c64, const int32_t* cell_map, const void* X0, double tol, int itermax,
+                   int max_outer, void* X, void* diag_out, void* eper_out, double* obs, int* iter_fin,
+                   double* err_fin, double* history, void* work, size_t work_bytes, void* stream);
 
 /* ---- GRE lattice occupancy (shape_model/gaussian_ellipsoid.py:182-237) -------
  * replaces find_nearest_distance_from_the_GRE_surf (:182-192, a k-d tree

@@ -114,7 +114,8 @@ def gre_geometry(ge, r_v_base, bc, ab, beta, seed, lattice_lf=None):
     axes = (g3[:, 0, 0, 0].copy(), g3[0, :, 0, 1].copy(), g3[0, 0, :, 2].copy())
     return dict(name=gre.name, lattice_n=np.asarray(lattice_n, dtype=np.int64),
                 lattice_lf=float(gre.lattice_lf), grid=grid, is_in=np.asarray(is_in, bool),
-                x_axis=axes[0], y_axis=axes[1], z_axis=axes[2])
+                x_axis=axes[0], y_axis=axes[1], z_axis=axes[2], surface=r_pts,
+                thr=float(gre.distance_factor * gre.lattice_lf))
 
 
 def geometry_record(geo) -> dict:
@@ -282,7 +283,11 @@ def small_fixtures(mf, bk, sc, ge) -> dict:
     # --- config 2 geometry --------------------------------------------------------
     geo, wl_0, m_m = cfg2_geometry(ge)
     rec = geometry_record(geo)
-    rec.update(euler=so3_euler(64, 2), wl_0=wl_0, m_m=m_m, m_p_xyz=CFG2_M_P)
+    # the reference's surface points and near-surface threshold: the surface
+    # comes from LAPACK's eigh, whose last bits vary with the CPU's code path,
+    # so the lattice occupancy is checked from these on any machine
+    rec.update(euler=so3_euler(64, 2), wl_0=wl_0, m_m=m_m, m_p_xyz=CFG2_M_P, surface=geo["surface"],
+               thr=geo["thr"])
     out["geometry_cfg2"] = rec
     return out
 
@@ -330,6 +335,16 @@ def sweep_small_fixture(sc, ge, mie) -> dict:
                                                                       lattice_n, dist)
                     r_ve = np.cbrt(3.0 * gre.lattice_lf ** 3 * int(is_in.sum()) / (4 * np.pi))
                     out["r_ve"][s4] = r_ve
+                    nx, ny, nz = (int(v) for v in lattice_n)
+                    g3 = grid.reshape(nx, ny, nz, 3)
+                    tag = "shape_%d_%d_%d_%d_" % s4
+                    out[tag + "lattice_n"] = np.asarray(lattice_n, dtype=np.int64)
+                    out[tag + "lattice_lf"] = float(gre.lattice_lf)
+                    out[tag + "x_axis"] = g3[:, 0, 0, 0].copy()
+                    out[tag + "y_axis"] = g3[0, :, 0, 1].copy()
+                    out[tag + "z_axis"] = g3[0, 0, :, 2].copy()
+                    out[tag + "mask_bits"] = np.packbits(np.asarray(is_in, bool))
+                    out[tag + "name"] = gre.name
                     for i_pair, (wl_0, m_m) in enumerate(sp["wl_m_m_pairs"]):
                         for i_mp, m_p_xyz in enumerate(sp["m_p_xyz_list"]):
                             idx6 = (i_pair, i_mp) + s4

@@ -76,3 +76,54 @@ def test_non_absorbing_particle_has_zero_c_abs_and_unconverged_is_zero():
     dd2.solve_matrix_equation()
     assert not dd2.converge
     assert np.all(dd2.compute_C_ext() == 0.0)      # P stays zero, as in the reference
+
+
+@pytest.mark.parametrize("solver,precision", [("bicgstab", None), ("cocg", None), ("bicgstab", "mixed"),
+                                              ("bicgstab", "c64")])
+def test_fused_solve_matches_the_separate_steps(solver, precision):
+    """bdda_dda_solve (right-hand side formed in the prologue, observables in the
+    epilogue) against polarizability + RHS kernels, the bl_krylov solver and the
+    observables kernel run one after another on the same inputs."""
+    from bl_krylov import bl_krylov as bk
+    rec = load_geometry(os.path.join(GOLDEN, "geometry_cfg1.npz"))
+    dd = _dd(rec)
+    dd.tol, dd.itermax, dd.solver, dd.precision = 1e-6, 300, solver, precision
+    dd.set_interaction_matrix()
+    dd.solve_matrix_equation()
+    obs_fused = dd.observables().copy()
+    ref = _dd(rec)
+    ref.set_interaction_matrix(green=dd.Au_til)
+    ref._materialize()
+    fn = bk.bl_cocg_rq_jacobi_mvp_fft if solver == "cocg" else bk.bl_bicgstab_jacobi_mvp_fft
+    X, it, err = fn(ref.lattice_n, 3, ref._dev["occ"], ref.Au_til, ref._dev["diag"], ref._dev["B"], 1e-6, 300,
+                    precision=precision)
+    assert it == dd.iter_fin and abs(err - dd.err_fin) <= 1e-12 * err
+    assert rel(dd.X, X.cpu().numpy()) < 1e-12
+    ref._dev["X"] = X
+    ref.converge = True
+    assert rel(obs_fused, ref.observables()) < 1e-12
+    assert rel(dd.diag_A, ref.diag_A) == 0.0 and rel(dd.eper_r, ref.eper_r) == 0.0
+
+
+def test_more_than_64_orientations_are_solved_in_blocks():
+    """L = 70: two blocks of 35 through the fused entry point, each the same as
+    a solve of those 35 orientations alone."""
+    from bdda_b200.inputs import so3_euler
+    from bl_dda import scatterer as sc
+    rec = load_geometry(os.path.join(GOLDEN, "kat_test_dda.npz"))
+    euler = so3_euler(70, 9)
+    sc.DiscreteDipoles.verbose = False
+    target = sc.Target("gre", rec["lattice_n"], rec["lattice_lf"], rec["grid"], rec["is_in"], rec["m_p_xyz"])
+    dd = sc.DiscreteDipoles(target, sc.IncidentField(float(rec["wl_0"]), float(rec["m_m"]), euler))
+    dd.tol, dd.itermax = 1e-6, 200
+    dd.set_interaction_matrix()
+    dd.solve_matrix_equation()
+    assert dd.converge and dd.X.shape == (3 * rec["address"].size, 70)
+    obs = dd.observables()
+    for l0, l1 in ((0, 35), (35, 70)):
+        d = sc.DiscreteDipoles(target, sc.IncidentField(float(rec["wl_0"]), float(rec["m_m"]), euler[l0:l1]))
+        d.tol, d.itermax = 1e-6, 200
+        d.set_interaction_matrix(green=dd.Au_til)
+        d.solve_matrix_equation()
+        assert rel(dd.X[:, l0:l1], d.X) < 1e-13
+        assert rel(obs[l0:l1], d.observables()) < 1e-13

@@ -126,17 +126,35 @@ def test_sweep_refuses_a_folder_of_another_sweep(tmp_path, monkeypatch):
         S.Sweep(_spec(num_orientations=16), out, solve=_FakeSolver(), verbose=False)
 
 
+def _golden_geometry(g):
+    """gre_geometry stand-in serving the reference's own lattices of the small sweep
+    (the GRE surface depends on the host's LAPACK eigh, so it is not redrawn here)."""
+    from bdda_b200.inputs import lattice_points
+
+    def geometry(r_v_base, bc, ab, beta, seed, lattice_lf=None, mask_fn=None):
+        i = int(np.flatnonzero(np.isclose(g["r_v_base_list"], r_v_base))[0])
+        tag = "shape_%d_0_0_0_" % i
+        n = g[tag + "lattice_n"]
+        is_in = np.unpackbits(g[tag + "mask_bits"])[:int(np.prod(n))].astype(bool)
+        lf = float(g[tag + "lattice_lf"])
+        return dict(name=str(g[tag + "name"]), lattice_n=n, lattice_lf=lf, is_in=is_in,
+                    address=np.flatnonzero(is_in),
+                    grid=lattice_points(g[tag + "x_axis"], g[tag + "y_axis"], g[tag + "z_axis"]),
+                    r_ve=float(np.cbrt(3.0 * lf ** 3 * int(is_in.sum()) / (4 * np.pi))))
+    return geometry
+
+
 @pytest.mark.gpu
-def test_small_sweep_matches_reference_run(tmp_path):
-    """The sweep on the GPU (batched solves, lattices built by the GPU
-    near-surface kernel) against the same sweep run with the reference's
-    classes: same angles and r_ve, observables of these short solves (tol
-    1e-2, a few iterations) to 1e-8, Mie values to the reference's complex64
-    rounding."""
-    from bdda_b200.geometry import inside_from_gpu
+def test_small_sweep_matches_reference_run(tmp_path, monkeypatch):
+    """The sweep on the GPU (batched solves, Green's spectra shared across m_p)
+    on the reference's own lattices, against the same sweep run with the
+    reference's classes: same angles and r_ve, observables of these short
+    solves (tol 1e-2, a few iterations) to 1e-8, Mie values to the
+    reference's complex64 rounding."""
     g = load_golden("sweep_small")
+    monkeypatch.setattr(S, "gre_geometry", _golden_geometry(g))
     out = str(tmp_path / "sweep")
-    sw = S.Sweep(_spec(), out, mask_fn=inside_from_gpu, verbose=False)
+    sw = S.Sweep(_spec(), out, verbose=False)
     assert sw.run() == 8
     r = S.load_results(out)
     assert r["done"].all() and r["converged"].all()
