@@ -539,6 +539,212 @@ def run_mvp_only(args):
 
 
 # ---------------------------------------------------------------------------
+# one large particle: plain FP64 vs the mixed form, with the roofline of this grid
+# ---------------------------------------------------------------------------
+CFG5 = dict(x=30.0, ab=1 / 0.6, bc=1 / 0.75, beta=0.15, seed=5, wl_0=1.0, m_m=1.0, ppl=14.0,
+            m_p=(1.58 + 0.003j, 1.66 + 0.003j, 1.55 + 0.004j), L=64, euler_seed=5)
+
+
+def _peak_hbm():
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except (OSError, ValueError):
+        peaks = {}
+    return float(peaks.get("hbm_gbs", 6650.0)), ("measured" if "hbm_gbs" in peaks else "fallback")
+
+
+def _obs_errs(o, r):
+    out = {}
+    for name, cols in (("C_ext", (1,)), ("S_fw_theta", (2, 3)), ("S_fw_phi", (4, 5)), ("S_bk", (10, 11))):
+        a = o[:, cols[0]] + (1j * o[:, cols[1]] if len(cols) > 1 else 0)
+        b = r[:, cols[0]] + (1j * r[:, cols[1]] if len(cols) > 1 else 0)
+        out[name] = float("%.3g" % (np.max(np.abs(a - b)) / np.max(np.abs(b))))
+    return out
+
+
+def run_large(args):
+    """The large birefringent particle: GRE x = 30, axis ratios 1/0.6 and 1/0.75
+    (the reciprocals of the literal 0.6 / 0.75, whose lattice is 2 % filled and
+    whose doubled complex128 field at L = 64 would need ~500 GB), beta 0.15,
+    surface seed 5, m_m 1, spacing lambda/14, L = 64: the plain complex128
+    solve and the mixed form at the accuracy-gate tolerance, their observables
+    against a converged complex128 solve, the peak device memory, and the
+    per-pass roofline of this grid's products (run-time-radix kernels)."""
+    import torch
+    from bdda_b200 import _lib
+    from bdda_b200.geometry import inside_from_gpu
+    from bdda_b200.inputs import so3_euler
+    from bdda_b200.runtime import autotune
+    from bdda_b200.shapes import gre_particle
+    from bl_dda import scatterer as sc
+    sc.DiscreteDipoles.verbose = False
+    c = CFG5
+    t0 = time.perf_counter()
+    geo = gre_particle(c["x"], c["ab"], c["bc"], c["beta"], c["seed"], wl_0=c["wl_0"], m_m=c["m_m"], ppl=c["ppl"],
+                       mask_fn=inside_from_gpu)
+    geo_s = time.perf_counter() - t0
+    L = c["L"]
+    euler = so3_euler(L, c["euler_seed"])
+    lib = _lib.load()
+    tol = args.tol
+
+    def make(prec, tol_):
+        t = sc.Target("gre30", geo["lattice_n"], geo["lattice_lf"], geo["grid"], geo["is_in"], list(c["m_p"]))
+        d = sc.DiscreteDipoles(t, sc.IncidentField(c["wl_0"], c["m_m"], euler))
+        d.tol, d.itermax, d.precision = tol_, ITERMAX, prec
+        return d
+    d0 = make(None, tol)
+    t0 = time.perf_counter()
+    d0.set_interaction_matrix()
+    torch.cuda.synchronize()
+    green_s = time.perf_counter() - t0
+    green = d0.Au_til
+    t0 = time.perf_counter()
+    tuned = {p: autotune(green, d0._dev["occ"], L, p, reps=2) for p in ("c128", "c64")}
+    tune_s = time.perf_counter() - t0
+
+    def step(d):
+        d.set_interaction_matrix(green=green)
+        d.solve_matrix_equation()
+        return d.observables()
+
+    def timed(d, steps):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            o = step(d)
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps, o
+
+    res = {}
+    peak, peak_src = _peak_hbm()
+    for name, prec in (("fp64", None), ("mixed", "mixed")):
+        d = make(prec, tol)
+        step(d)   # warm-up
+        torch.cuda.reset_peak_memory_stats()
+        lib.bdda_profile_enable(1)
+        ms, obs = timed(d, max(1, args.steps))
+        prof = {}
+        for pc in (_lib.C128, _lib.C64):
+            pm = (_lib.C.c_double * 5)()
+            nm = _lib.C.c_longlong(0)
+            lib.bdda_profile_read(pc, pm, _lib.C.byref(nm))
+            if nm.value:
+                prof[pc] = ([pm[i] / nm.value for i in range(5)], nm.value)
+        lib.bdda_profile_enable(0)
+        lines = {}
+        for pc, (per, cnt) in prof.items():
+            pb = mvp_pass_bytes(green.plan.n, green.plan.m, d.num_element_occupy, L, 16 if pc == _lib.C128 else 8)
+            lines["complex128" if pc == _lib.C128 else "complex64"] = {
+                "mvp_ms": round(sum(per), 3), "mvps_timed": cnt, "alg_bytes_per_mvp": int(sum(pb)),
+                "achieved_GBs": round(sum(pb) / (sum(per) * 1e-3) / 1e9, 1),
+                "frac": round(sum(pb) / (sum(per) * 1e-3) / 1e9 / peak, 3),
+                "passes_frac": [round(b / (t * 1e-3) / 1e9 / peak, 3) for b, t in zip(pb, per)]}
+        res[name] = dict(value=round(L / (ms * 1e-3), 3), ms_per_step=round(ms, 1), iterations=d.iter_fin + 1,
+                         err_fin=d.err_fin, converged=d.converge, peak_device_GB=round(
+                             torch.cuda.max_memory_allocated() / 1e9, 2), products=lines, obs=obs)
+        del d
+        torch.cuda.empty_cache()
+    dref = make(None, 1e-9)
+    dref.itermax = 1000
+    oref = step(dref)
+    del dref
+    err_mf = _obs_errs(res["mixed"]["obs"], res["fp64"]["obs"])
+    out = {"metric": "orientations/s, large birefringent particle, plain FP64 vs mixed form", "unit": "orientations/s",
+           "config": {"workload": "GRE x=30, ab 1/0.6, bc 1/0.75, beta 0.15, seed 5, m_m 1, lambda/14, m_p "
+                                  "(1.58+0.003i, 1.66+0.003i, 1.55+0.004i), L=64 SO(3) orientations (seed 5), "
+                                  "block-BiCGSTAB to %g" % tol,
+                      "instance": "reciprocal axis ratios (1/0.6, 1/0.75): the literal 0.6 / 0.75 lattice is "
+                                  "222x330x279 with 2% fill",
+                      "lattice": [int(v) for v in geo["lattice_n"]], "grid": list(green.plan.m),
+                      "radices": [green.plan.radices(a) for a in range(3)],
+                      "n_dipoles": int(geo["address"].size), "tol": tol},
+           "fp64": {k: v for k, v in res["fp64"].items() if k != "obs"},
+           "mixed": {k: v for k, v in res["mixed"].items() if k != "obs"},
+           "speedup_of_mixed": round(res["fp64"]["ms_per_step"] / res["mixed"]["ms_per_step"], 3),
+           "max_rel_err_mixed_vs_fp64": err_mf, "accuracy_ok": bool(max(err_mf.values()) <= 1e-4),
+           "max_rel_err_vs_converged_fp64": {"mixed": _obs_errs(res["mixed"]["obs"], oref),
+                                             "fp64": _obs_errs(res["fp64"]["obs"], oref)},
+           "peak_hbm": {"GBs": peak, "source": peak_src},
+           "setup_s": {"geometry_host_plus_gpu_mask": round(geo_s, 2), "green": round(green_s, 3),
+                       "autotune": round(tune_s, 2)},
+           "autotune_mvp_ms": {k: [round(v[0], 3), round(v[1], 3)] for k, v in tuned.items()}}
+    print(json.dumps(out), flush=True)
+
+
+def run_sphere(args):
+    """The small sphere (x = 5, m 1.5+0.01i, lambda/16 -> 28^3 lattice, L = 8,
+    seed 0, block-COCG-rq to 1e-5): orientations/s of the complex128 path, its
+    iterations and outputs against the reference's own solve of this case
+    (tests/golden/geometry_cfg1.npz), the Mie check of the volume-equivalent
+    sphere, and the reference's algorithm (the oracle) on the host cores."""
+    import torch
+    from bdda_b200.inputs import load_geometry
+    from bdda_b200.mie import mie_q_and_s
+    from bl_dda import scatterer as sc
+    sc.DiscreteDipoles.verbose = False
+    path = os.path.join(REPO, "tests", "golden", "geometry_cfg1.npz")
+    geo = load_geometry(path)
+    ref = dict(np.load(path, allow_pickle=False))
+    t = sc.Target("sphere", geo["lattice_n"], geo["lattice_lf"], geo["grid"], geo["is_in"], geo["m_p_xyz"])
+    d = sc.DiscreteDipoles(t, sc.IncidentField(float(geo["wl_0"]), float(geo["m_m"]), geo["euler"]))
+    d.tol, d.itermax, d.solver = TOL, 300, "cocg"
+    d.set_interaction_matrix()
+    green = d.Au_til
+
+    def step():
+        d.set_interaction_matrix(green=green)
+        d.solve_matrix_equation()
+        return d.observables()
+    for _ in range(max(3, args.warmup)):
+        step()
+    steps = max(10, args.steps)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        obs = step()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    L = obs.shape[0]
+    errs = {}
+    for name, cols in (("C_ext", (1,)), ("S_fw_theta", (2, 3)), ("S_fw_phi", (4, 5)), ("S_bk", (10, 11))):
+        a = obs[:, cols[0]] + (1j * obs[:, cols[1]] if len(cols) > 1 else 0)
+        errs[name] = float("%.3g" % (np.max(np.abs(a - ref[name])) / np.max(np.abs(ref[name]))))
+    r_ve = float(d.ve_radius)
+    _, q_abs, q_ext, _, _ = mie_q_and_s(float(geo["wl_0"]), float(geo["m_m"]), r_ve, complex(geo["m_p_xyz"][0]))
+    q_dda = float(np.mean(obs[:, 1])) / (np.pi * r_ve ** 2)
+    from oracle import dda_oracle as O
+    O.FFT_WORKERS = os.cpu_count() or 1
+    g = O.incident_geometry(float(geo["wl_0"]), float(geo["m_m"]), geo["euler"])
+    Ghat = O.fft_init(geo["lattice_n"], 3, geo["lattice_lf"], g["k"])
+    t0 = time.perf_counter()
+    eper_r, _, diag = O.polarizability(geo["m_p_xyz"], float(geo["m_m"]), geo["lattice_lf"], g["k"],
+                                       geo["address"].size)
+    B = O.rhs(g["k"], g["u_inc"], g["e0_inc"], geo["grid"][geo["address"]])
+    Xo, ito, _ = O.cocg_rq(geo["lattice_n"], 3, geo["address"], Ghat, diag, B, TOL, 300)
+    O.observables(Xo, g, geo["grid"][geo["address"]], eper_r, geo["lattice_lf"])
+    cpu_s = time.perf_counter() - t0
+    out = {"metric": "orientations/s, small sphere, plain FP64 (block-COCG-rq to 1e-5)", "unit": "orientations/s",
+           "value": round(L / (ms * 1e-3), 2), "ms_per_step": round(ms, 3), "steps": steps,
+           "config": {"workload": "sphere x=5 (wl 1, m_m 1), m_p 1.5+0.01i, lambda/16 -> 28^3 lattice, "
+                                  "%d dipoles, L=8 SO(3) orientations (seed 0), block-COCG-rq to 1e-5"
+                                  % geo["address"].size},
+           "iterations": d.iter_fin + 1, "reference_iterations": int(ref["iter_fin"]) + 1,
+           "max_rel_err_vs_reference_solve": errs,
+           "mie": {"Q_ext_dda_mean": round(q_dda, 5), "Q_ext_mie": round(q_ext, 5),
+                   "rel_diff": round(abs(q_dda / q_ext - 1), 5)},
+           "cpu_baseline": {"value": round(L / cpu_s, 4), "unit": "orientations/s", "cores": O.FFT_WORKERS,
+                            "kind": "port", "sample": "oracle: RHS + block-COCG-rq %d iterations + observables, "
+                                                      "whole solve %.2fs" % (ito + 1, cpu_s)}}
+    print(json.dumps(out), flush=True)
+
+
+# ---------------------------------------------------------------------------
 # batched uneven sweep: 48 GRE particles x 3 wavelengths, L = 32
 # ---------------------------------------------------------------------------
 SWEEP_WL = (0.45, 0.55, 0.85)
@@ -767,6 +973,10 @@ def main():
     ap.add_argument("--sweep-particles", type=int, default=48)
     ap.add_argument("--sweep-arms", default="one_at_a_time_fp64,batched_fp64,batched_mixed")
     ap.add_argument("--sweep-x", default="4,16", help="size-parameter range of the sweep particles")
+    ap.add_argument("--large", action="store_true",
+                    help="the large birefringent particle (x=30, 215x129x106 lattice): FP64 vs mixed")
+    ap.add_argument("--sphere", action="store_true",
+                    help="the small sphere (x=5, 28^3, L=8, COCG-rq): FP64 against the reference's solve and Mie")
     ap.add_argument("--fno", action="store_true", help="train and evaluate the learned warm start")
     ap.add_argument("--fno-train", type=int, default=256)
     ap.add_argument("--fno-eval", type=int, default=32)
@@ -776,6 +986,12 @@ def main():
     ap.add_argument("--fno-save", default=None)
     ap.add_argument("--fno-verbose", action="store_true")
     args = ap.parse_args()
+    if args.large:
+        run_large(args)
+        return
+    if args.sphere:
+        run_sphere(args)
+        return
     if args.fno:
         run_fno(args)
         return

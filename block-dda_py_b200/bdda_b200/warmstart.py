@@ -108,7 +108,7 @@ class WarmStartFNO:
         return w
 
     def supports(self, n) -> bool:
-        return all(self.cfg.modes <= int(v) <= 128 for v in n)
+        return all(self.cfg.modes <= int(v) <= 512 for v in n)
 
     def buffer(self, work, L, n, which, count, dtype=torch.float32):
         off = int(_lib.load().bdda_fno_buffer_offset(C.byref(self.cfg), int(L), _n3(n), which))

@@ -25,6 +25,10 @@ struct FnoCfg {
   int cin, width, cout, proj, layers, modes;
 };
 
+// Longest lattice axis the network runs on (its truncated-DFT tables hold
+// kMaxAxis x modes entries per axis).
+constexpr int kMaxAxis = 512;
+
 // parameter offsets (floats)
 struct FnoParams {
   size_t P, p, R[8], W[8], b[8], Q1, q1, Q2, q2, total;
@@ -269,6 +273,257 @@ __global__ void __launch_bounds__(256) pointwise_bwd_weight_kernel(const float* 
   }
 }
 
+// ---- tensor-core pointwise layers --------------------------------------------------------------
+// The CI x CO maps whose sides are multiples of 8 (the width x width layers and
+// the first projection) run on the tensor cores: mma.sync m16n8k8 with TF32
+// operands and FP32 accumulation, each product split in three,
+// a b ~ a_hi b_hi + a_hi b_lo + a_lo b_hi with a_hi = tf32(a), a_lo = tf32(a - a_hi),
+// which keeps the accuracy of the FP32 kernels (the dropped a_lo b_lo term is
+// below FP32 rounding).  Fragments of m16n8k8 (lane = 4 g + t):
+// A (16 x 8) a0 (g, t), a1 (g + 8, t), a2 (g, t + 4), a3 (g + 8, t + 4);
+// B (8 x 8) b0 (t, g), b1 (t + 4, g); D (16 x 8) d0 (g, 2t), d1 (g, 2t + 1),
+// d2 (g + 8, 2t), d3 (g + 8, 2t + 1).  Each warp owns 16-row tiles of the
+// activations, staged in shared memory by 16-byte loads.
+__device__ __forceinline__ uint32_t tf32_of(float v) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(v));
+  return r;
+}
+__device__ __forceinline__ void split_tf32(float v, uint32_t& hi, uint32_t& lo) {
+  hi = tf32_of(v);
+  lo = tf32_of(v - __uint_as_float(hi));
+}
+__device__ __forceinline__ void mma_tf32(float* d, const uint32_t* a, const uint32_t* b) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+// d += A B over K = 8 KS columns: A from a 16-row tile at `at` (row stride AS),
+// B fragments from split matrices bh / bl (row k, column n, row stride BS)
+template <int KS, int NS, int AS, int BS>
+__device__ __forceinline__ void tile_mma(float (*acc)[4], const float* at, const uint32_t* bh, const uint32_t* bl,
+                                         int g, int t) {
+#pragma unroll
+  for (int ks = 0; ks < KS; ++ks) {
+    uint32_t ah[4], al[4];
+    split_tf32(at[g * AS + ks * 8 + t], ah[0], al[0]);
+    split_tf32(at[(g + 8) * AS + ks * 8 + t], ah[1], al[1]);
+    split_tf32(at[g * AS + ks * 8 + t + 4], ah[2], al[2]);
+    split_tf32(at[(g + 8) * AS + ks * 8 + t + 4], ah[3], al[3]);
+#pragma unroll
+    for (int ns = 0; ns < NS; ++ns) {
+      const int wi = (ks * 8 + t) * BS + ns * 8 + g;
+      const uint32_t h[2] = {bh[wi], bh[wi + 4 * BS]}, l[2] = {bl[wi], bl[wi + 4 * BS]};
+      mma_tf32(acc[ns], al, h);
+      mma_tf32(acc[ns], ah, l);
+      mma_tf32(acc[ns], ah, h);
+    }
+  }
+}
+
+// stage rows m0 .. m0+R-1 of a row-major (M x C) array into a tile of row stride TS (zero past M)
+template <int R, int C, int TS>
+__device__ __forceinline__ void stage_rows(const float* src, int64_t m0, int64_t M, float* tile, int lane) {
+  for (int e = lane; e < R * C / 4; e += 32) {
+    const int r = e / (C / 4), c4 = e - r * (C / 4);
+    float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (m0 + r < M) v = *reinterpret_cast<const float4*>(src + (m0 + r) * C + 4 * c4);
+    float* d = tile + r * TS + 4 * c4;
+    d[0] = v.x; d[1] = v.y; d[2] = v.z; d[3] = v.w;
+  }
+}
+
+// as pointwise_fwd_kernel: z = x Wt + bias (+ add), y = act(z)
+template <int CI, int CO>
+__global__ void __launch_bounds__(256) pointwise_fwd_tc_kernel(const float* x, const float* Wt, const float* bias,
+                                                               const float* add, float* z, float* y, int64_t M,
+                                                               int act) {
+  static_assert(CI % 8 == 0 && CO % 8 == 0 && CI <= 64 && CO <= 64, "tensor-core tile shapes");
+  constexpr int WS = CO + 8, XS = CI + 4;   // padded strides: conflict-free fragment reads
+  __shared__ uint32_t wh[CI * WS], wl[CI * WS];
+  __shared__ __align__(16) float xs[8][16 * XS];
+  __shared__ float bs[CO];
+  for (int e = threadIdx.x; e < CI * CO; e += blockDim.x) {
+    const int i = e / CO, o = e - i * CO;
+    split_tf32(Wt[e], wh[i * WS + o], wl[i * WS + o]);
+  }
+  for (int e = threadIdx.x; e < CO; e += blockDim.x) bs[e] = bias[e];
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  float* xt = xs[warp];
+  const int64_t ntile = (M + 15) / 16;
+  for (int64_t tile = blockIdx.x * 8LL + warp; tile < ntile; tile += (int64_t)gridDim.x * 8) {
+    const int64_t m0 = tile * 16;
+    stage_rows<16, CI, XS>(x, m0, M, xt, lane);
+    __syncwarp();
+    float acc[CO / 8][4];
+#pragma unroll
+    for (int ns = 0; ns < CO / 8; ++ns) acc[ns][0] = acc[ns][1] = acc[ns][2] = acc[ns][3] = 0.f;
+    tile_mma<CI / 8, CO / 8, XS, WS>(acc, xt, wh, wl, g, t);
+    __syncwarp();
+#pragma unroll
+    for (int ns = 0; ns < CO / 8; ++ns) {
+#pragma unroll
+      for (int hr = 0; hr < 2; ++hr) {
+        const int64_t m = m0 + g + 8 * hr;
+        if (m >= M) continue;
+        const int o = ns * 8 + 2 * t;
+        float v0 = acc[ns][2 * hr] + bs[o], v1 = acc[ns][2 * hr + 1] + bs[o + 1];
+        if (add) {
+          const float2 a2 = *reinterpret_cast<const float2*>(add + m * CO + o);
+          v0 += a2.x;
+          v1 += a2.y;
+        }
+        if (z) *reinterpret_cast<float2*>(z + m * CO + o) = make_float2(v0, v1);
+        *reinterpret_cast<float2*>(y + m * CO + o) = act ? make_float2(gelu(v0), gelu(v1)) : make_float2(v0, v1);
+      }
+    }
+  }
+}
+
+// as pointwise_bwd_data_kernel: gz = gy act'(z) (stored); gx = gz Wt^T (set or added)
+template <int CI, int CO>
+__global__ void __launch_bounds__(128) pointwise_bwd_data_tc_kernel(const float* gy, const float* z, const float* Wt,
+                                                                    float* gz, float* gx, int64_t M, int act,
+                                                                    int accumulate) {
+  static_assert(CI % 8 == 0 && CO % 8 == 0 && CI <= 64 && CO <= 64, "tensor-core tile shapes");
+  constexpr int WS = CI + 8, GS = CO + 4, NW = 4;
+  __shared__ uint32_t wh[CO * WS], wl[CO * WS];   // W transposed: row o, column i
+  __shared__ __align__(16) float gsm[NW][16 * GS];
+  for (int e = threadIdx.x; e < CI * CO; e += blockDim.x) {
+    const int i = e / CO, o = e - i * CO;
+    split_tf32(Wt[e], wh[o * WS + i], wl[o * WS + i]);
+  }
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  float* gt = gsm[warp];
+  const int64_t ntile = (M + 15) / 16;
+  for (int64_t tile = blockIdx.x * (int64_t)NW + warp; tile < ntile; tile += (int64_t)gridDim.x * NW) {
+    const int64_t m0 = tile * 16;
+    for (int e = lane; e < 16 * CO / 4; e += 32) {   // gz tile = gy act'(z), written back
+      const int r = e / (CO / 4), c4 = e - r * (CO / 4);
+      float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (m0 + r < M) {
+        const int64_t off = (m0 + r) * CO + 4 * c4;
+        v = *reinterpret_cast<const float4*>(gy + off);
+        if (act) {
+          const float4 zz = *reinterpret_cast<const float4*>(z + off);
+          v.x *= gelu_grad(zz.x); v.y *= gelu_grad(zz.y); v.z *= gelu_grad(zz.z); v.w *= gelu_grad(zz.w);
+        }
+        *reinterpret_cast<float4*>(gz + off) = v;
+      }
+      float* d = gt + r * GS + 4 * c4;
+      d[0] = v.x; d[1] = v.y; d[2] = v.z; d[3] = v.w;
+    }
+    __syncwarp();
+    if (gx) {
+      float acc[CI / 8][4];
+#pragma unroll
+      for (int ns = 0; ns < CI / 8; ++ns) acc[ns][0] = acc[ns][1] = acc[ns][2] = acc[ns][3] = 0.f;
+      tile_mma<CO / 8, CI / 8, GS, WS>(acc, gt, wh, wl, g, t);
+#pragma unroll
+      for (int ns = 0; ns < CI / 8; ++ns) {
+#pragma unroll
+        for (int hr = 0; hr < 2; ++hr) {
+          const int64_t m = m0 + g + 8 * hr;
+          if (m >= M) continue;
+          float2* dst = reinterpret_cast<float2*>(gx + m * CI + ns * 8 + 2 * t);
+          float2 v = make_float2(acc[ns][2 * hr], acc[ns][2 * hr + 1]);
+          if (accumulate) {
+            const float2 o = *dst;
+            v.x += o.x;
+            v.y += o.y;
+          }
+          *dst = v;
+        }
+      }
+    }
+    __syncwarp();
+  }
+}
+
+// as pointwise_bwd_weight_kernel: gWt += x^T gz, gb += column sums of gz.  K
+// runs over the rows: each warp takes 16-row blocks of this CTA's row range,
+// A = x^T (CI x 8 per step), B = gz (8 x CO); warps meet in shared memory,
+// then one atomic add per element per CTA.
+template <int CI, int CO>
+__global__ void __launch_bounds__(128) pointwise_bwd_weight_tc_kernel(const float* x, const float* gz, float* gWt,
+                                                                      float* gb, int64_t M) {
+  static_assert(CI % 16 == 0 && CO % 8 == 0 && CI <= 64 && CO <= 64, "tensor-core tile shapes");
+  constexpr int XS = CI + 8, GS = CO + 8, NW = 4, RB = 16;   // row = sample m; RB rows per warp block
+  __shared__ __align__(16) float xs[NW][RB * XS];
+  __shared__ __align__(16) float gs[NW][RB * GS];
+  __shared__ float red[CI * CO + CO];
+  for (int e = threadIdx.x; e < CI * CO + CO; e += blockDim.x) red[e] = 0.f;
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  float* xt = xs[warp];
+  float* gt = gs[warp];
+  const int64_t rows_per = (M + gridDim.x - 1) / gridDim.x;
+  const int64_t r0 = blockIdx.x * rows_per, r1 = min(M, r0 + rows_per);
+  float acc[CI / 16][CO / 8][4];
+#pragma unroll
+  for (int mt = 0; mt < CI / 16; ++mt)
+#pragma unroll
+    for (int ns = 0; ns < CO / 8; ++ns) acc[mt][ns][0] = acc[mt][ns][1] = acc[mt][ns][2] = acc[mt][ns][3] = 0.f;
+  float bsum[(CO + 31) / 32];
+#pragma unroll
+  for (int q = 0; q < (CO + 31) / 32; ++q) bsum[q] = 0.f;
+  for (int64_t rb = r0 + (int64_t)RB * warp; rb < r1; rb += (int64_t)RB * NW) {
+    stage_rows<RB, CI, XS>(x, rb, r1, xt, lane);
+    stage_rows<RB, CO, GS>(gz, rb, r1, gt, lane);
+    __syncwarp();
+#pragma unroll
+    for (int ks = 0; ks < RB / 8; ++ks) {   // 8 samples per step
+      const int k0 = ks * 8;
+      uint32_t bh[CO / 8][2], bl[CO / 8][2];
+#pragma unroll
+      for (int ns = 0; ns < CO / 8; ++ns) {
+        split_tf32(gt[(k0 + t) * GS + ns * 8 + g], bh[ns][0], bl[ns][0]);
+        split_tf32(gt[(k0 + t + 4) * GS + ns * 8 + g], bh[ns][1], bl[ns][1]);
+      }
+#pragma unroll
+      for (int mt = 0; mt < CI / 16; ++mt) {
+        uint32_t ah[4], al[4];   // A[i][m] = x[m][i]
+        split_tf32(xt[(k0 + t) * XS + mt * 16 + g], ah[0], al[0]);
+        split_tf32(xt[(k0 + t) * XS + mt * 16 + g + 8], ah[1], al[1]);
+        split_tf32(xt[(k0 + t + 4) * XS + mt * 16 + g], ah[2], al[2]);
+        split_tf32(xt[(k0 + t + 4) * XS + mt * 16 + g + 8], ah[3], al[3]);
+#pragma unroll
+        for (int ns = 0; ns < CO / 8; ++ns) {
+          mma_tf32(acc[mt][ns], al, bh[ns]);
+          mma_tf32(acc[mt][ns], ah, bl[ns]);
+          mma_tf32(acc[mt][ns], ah, bh[ns]);
+        }
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < (CO + 31) / 32; ++q) {   // bias gradient: column sums
+      const int o = lane + 32 * q;
+      if (o < CO)
+        for (int r = 0; r < RB; ++r) bsum[q] += gt[r * GS + o];
+    }
+    __syncwarp();
+  }
+#pragma unroll
+  for (int q = 0; q < (CO + 31) / 32; ++q)
+    if (lane + 32 * q < CO) atomicAdd(&red[CI * CO + lane + 32 * q], bsum[q]);
+#pragma unroll
+  for (int mt = 0; mt < CI / 16; ++mt)
+#pragma unroll
+    for (int ns = 0; ns < CO / 8; ++ns)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int i = mt * 16 + g + 8 * (q >> 1), o = ns * 8 + 2 * t + (q & 1);
+        atomicAdd(&red[i * CO + o], acc[mt][ns][q]);
+      }
+  __syncthreads();
+  for (int e = threadIdx.x; e < CI * CO; e += blockDim.x) atomicAdd(&gWt[e], red[e]);
+  for (int e = threadIdx.x; e < CO; e += blockDim.x) atomicAdd(&gb[e], red[CI * CO + e]);
+}
+
 // ---- loss: masked relative squared error per sample -------------------------------------------
 // L = (1/B) sum_b sum_m mask |y - t|^2 / sum_m mask |t|^2 ; gy = dL/dy
 __global__ void loss_kernel(const float* y, const float* t, const float* mask, int64_t ncell, int C, int B,
@@ -468,7 +723,7 @@ FnoWork work_layout(const FnoCfg& c, const Shape& s) {
   w.gs = take(M * Wd * 4);
   w.gS = take((size_t)s.B * s.K * Wd * 8);
   w.gA = take((size_t)s.B * s.K * Wd * 8);
-  w.tabs = take((size_t)6 * 128 * 32 * 8);
+  w.tabs = take((size_t)6 * kMaxAxis * 32 * 8);
   w.mask = take(s.ncell * 4);
   w.tgt = take(M * c.cout * 4);
   w.gy = take(M * c.cout * 4);
@@ -502,7 +757,7 @@ int upload_tables(Ctx& x) {
   for (int t = 0; t < 6; ++t) {
     const int N = x.s.n[ax_of[t]];
     axis_table(N, md, t >= 3, T);
-    x.tab[t] = base + (size_t)t * 128 * 32;
+    x.tab[t] = base + (size_t)t * kMaxAxis * 32;
     BDDA_CUDA_TRY(cudaMemcpyAsync(x.tab[t], T.data(), T.size() * sizeof(float2), cudaMemcpyHostToDevice, x.st));
   }
   return BDDA_OK;
@@ -540,9 +795,21 @@ int dft_inv(Ctx& x, const float2* S, float* out, float scale, bool add) {
   return transform<true, 1>(x, t1, out, x.tab[5], (int64_t)B * Nx * Ny, md, Nz, W, scale);
 }
 
+// Layers whose sides are multiples of 8 (16 for the input side of the weight
+// gradient) run on the tensor cores; the lift (13 inputs) and the last
+// projection (6 outputs) keep the FP32 kernels.
+template <int CI, int CO>
+constexpr bool tc_shape() { return CI % 16 == 0 && CO % 8 == 0 && CI <= 64 && CO <= 64; }
+
 template <int CI, int CO>
 int pw_fwd(Ctx& x, const float* in, const float* Wt, const float* b, const float* add, float* z, float* y, int act) {
-  pointwise_fwd_kernel<CI, CO><<<grid_for(x.s.M), 256, 0, x.st>>>(in, Wt, b, add, z, y, x.s.M, act);
+  if constexpr (tc_shape<CI, CO>()) {
+    const int64_t tiles = (x.s.M + 15) / 16;
+    pointwise_fwd_tc_kernel<CI, CO><<<(int)std::min<int64_t>(148 * 8, (tiles + 7) / 8), 256, 0, x.st>>>(
+        in, Wt, b, add, z, y, x.s.M, act);
+  } else {
+    pointwise_fwd_kernel<CI, CO><<<grid_for(x.s.M), 256, 0, x.st>>>(in, Wt, b, add, z, y, x.s.M, act);
+  }
   count_launch();
   BDDA_CUDA_TRY(cudaGetLastError());
   return BDDA_OK;
@@ -550,9 +817,17 @@ int pw_fwd(Ctx& x, const float* in, const float* Wt, const float* b, const float
 template <int CI, int CO>
 int pw_bwd(Ctx& x, const float* gy, const float* z, const float* in, const float* Wt, float* gz, float* gx,
            float* gWt, float* gb, int act, int accumulate) {
-  pointwise_bwd_data_kernel<CI, CO><<<grid_for(x.s.M), 256, 0, x.st>>>(gy, z, Wt, gz, gx, x.s.M, act, accumulate);
-  pointwise_bwd_weight_kernel<CI, CO><<<std::min<int64_t>(148 * 4, (x.s.M + 255) / 256 + 1), 256, 0, x.st>>>(
-      in, gz, gWt, gb, x.s.M);
+  const int wgrid = (int)std::min<int64_t>(148 * 4, (x.s.M + 255) / 256 + 1);
+  if constexpr (tc_shape<CI, CO>()) {
+    const int64_t tiles = (x.s.M + 15) / 16;
+    pointwise_bwd_data_tc_kernel<CI, CO><<<(int)std::min<int64_t>(148 * 16, (tiles + 3) / 4), 128, 0, x.st>>>(
+        gy, z, Wt, gz, gx, x.s.M, act, accumulate);
+    pointwise_bwd_weight_tc_kernel<CI, CO><<<wgrid, 128, 0, x.st>>>(in, gz, gWt, gb, x.s.M);
+  } else {
+    pointwise_bwd_data_kernel<CI, CO><<<grid_for(x.s.M), 256, 0, x.st>>>(gy, z, Wt, gz, gx, x.s.M, act,
+                                                                         accumulate);
+    pointwise_bwd_weight_kernel<CI, CO><<<wgrid, 256, 0, x.st>>>(in, gz, gWt, gb, x.s.M);
+  }
   count_launch(2);
   BDDA_CUDA_TRY(cudaGetLastError());
   return BDDA_OK;
@@ -641,7 +916,7 @@ int make_ctx(Ctx& x, const bdda_fno_config* cfg, int B, const int n[3], void* wo
   x.pl = param_layout(x.c);
   x.s.B = B;
   for (int a = 0; a < 3; ++a) {
-    if (n[a] < x.c.modes || n[a] > 128) return BDDA_BAD_ARG;
+    if (n[a] < x.c.modes || n[a] > kMaxAxis) return BDDA_BAD_ARG;
     x.s.n[a] = n[a];
   }
   x.s.ncell = (int64_t)n[0] * n[1] * n[2];
@@ -654,7 +929,7 @@ int make_ctx(Ctx& x, const bdda_fno_config* cfg, int B, const int n[3], void* wo
   x.grad = grads;
   x.st = st;
   float2* base = at<float2>(x, x.wl.tabs);
-  for (int t = 0; t < 6; ++t) x.tab[t] = base + (size_t)t * 128 * 32;
+  for (int t = 0; t < 6; ++t) x.tab[t] = base + (size_t)t * kMaxAxis * 32;
   return tables ? upload_tables(x) : BDDA_OK;
 }
 

@@ -99,7 +99,7 @@ static int launch_lt(PassArgs a, int64_t P0, cudaStream_t st) {
 
 static int g_use_fixed = 1;   // specialised kernels on (bdda_tune_fixed)
 
-static constexpr int kFixedTables = 7;
+static constexpr int kFixedTables = 8;
 
 static const FixedKernel* fixed_table(int t, int* n) {
   switch (t) {
@@ -109,7 +109,8 @@ static const FixedKernel* fixed_table(int t, int* n) {
     case 3: return fixed_table_d(n);
     case 4: return fixed_table_e(n);
     case 5: return fixed_table_f(n);
-    default: return fixed_table_g(n);
+    case 6: return fixed_table_g(n);
+    default: return fixed_table_h(n);
   }
 }
 
@@ -169,6 +170,7 @@ static int launch_pass(const PassArgs& a, int64_t P0, int lt, cudaStream_t st) {
     if (f) return f(a, P0, st);
   }
   switch (lt) {
+    case 16:   // tile width 16 exists as specialised kernels only
     case 8: return launch_lt<T, KIND, 8>(a, P0, st);
     case 4: return launch_lt<T, KIND, 4>(a, P0, st);
     default: return launch_lt<T, KIND, 2>(a, P0, st);
@@ -315,12 +317,12 @@ static int autotune_impl(const bdda_plan* p, int L, const T* ghat, const int32_t
       Key key;
       key.kind = pass_kind[q];
       key.axis = pass_axis[q];
-      for (int lt : {8, 4, 2}) {
+      for (int lt : {16, 8, 4, 2}) {
         if (lt > 2 && lt / 2 >= L) continue;
         if (pencil_smem<T>(M, lt, key.kind) > 227 * 1024) continue;
         for (int v : fixed_variants(prec, key.kind, lt, p->ax[key.axis], pair_ok(pa[q])))
           key.cand.push_back({prec, key.kind, M, L, lt, v});
-        key.cand.push_back({prec, key.kind, M, L, lt, -1});
+        if (lt <= 8) key.cand.push_back({prec, key.kind, M, L, lt, -1});   // generic kernels go up to 8
       }
       key.ms.assign(key.cand.size(), 0.0);
       keys.push_back(key);

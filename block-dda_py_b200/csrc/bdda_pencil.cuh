@@ -437,6 +437,7 @@ const FixedKernel* fixed_table_d(int* n);
 const FixedKernel* fixed_table_e(int* n);
 const FixedKernel* fixed_table_f(int* n);
 const FixedKernel* fixed_table_g(int* n);
+const FixedKernel* fixed_table_h(int* n);
 
 
 }  // namespace bdda

@@ -311,7 +311,7 @@ int bdda_batch_bicgstab(const bdda_batch_problem* problems, int nprob, int mode,
  * complex width x width matrices on the `modes` lowest frequencies per axis,
  * plus a pointwise width x width map, GELU), projection width -> proj -> cout.
  * The shipped shapes are cin 13, width 32, cout 6, proj 64; every lattice
- * axis is at least `modes` and at most 128 cells.  One call handles B samples
+ * axis is at least `modes` and at most 512 cells.  One call handles B samples
  * (orientations) of one lattice; activations live in `work`
  * (bdda_fno_workspace_bytes), parameters in one FP32 array
  * (bdda_fno_param_count floats, layout by bdda_fno_offset).  bdda_fno_features
