@@ -950,7 +950,40 @@ def run_fno(args):
                      "seconds": round(train_s, 2), "data_generation_s": round(data_s, 2),
                      "shapes_host_s": round(shape_s, 2)},
            "per_particle": rows if args.fno_verbose else None}
+    if args.fno_headline:
+        out["headline_particle"] = _fno_on_headline(model)
     print(json.dumps(out), flush=True)
+
+
+def _fno_on_headline(model):
+    """The trained network on the headline particle (x = 20, 93 x 112 x 174, L = 64):
+    the mixed form at the accuracy-gate tolerance from zero and from the warm
+    start (inference and the fallback check inside the timed region)."""
+    import torch
+    from bl_dda import scatterer as sc
+    geo, euler = load_workload(64)
+    t = sc.Target("gre", geo["lattice_n"], geo["lattice_lf"], geo["grid"], geo["is_in"], geo["m_p_xyz"])
+    d = sc.DiscreteDipoles(t, sc.IncidentField(float(geo["wl_0"]), float(geo["m_m"]), euler))
+    d.tol, d.itermax, d.precision = TOL_GATE, ITERMAX, "mixed"
+    d.set_interaction_matrix()
+    d._materialize()
+    diag, B = d._dev["diag"], d._dev["B"]
+    eps = (np.asarray(geo["m_p_xyz"], dtype=np.complex128) / float(geo["m_m"])) ** 2
+    res = {}
+    for name in ("zero", "zero", "warm", "warm"):   # the first of each warms up
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        X0, nfb = (None, 0)
+        if name == "warm":
+            X0, nfb = model.warm_start(d.lattice_n, d._dev["occ"], d.Au_til, diag, B, eps)
+        d.set_interaction_matrix(green=d.Au_til)
+        d.solve_matrix_equation(X0=X0)
+        d.observables()
+        torch.cuda.synchronize()
+        res[name] = dict(seconds=round(time.perf_counter() - t0, 3), iterations=d.iter_fin + 1,
+                         converged=d.converge, fallback_columns=nfb)
+    return {"workload": "GRE x=20 (93x112x174, 438606 dipoles), L=64, mixed form to %g" % TOL_GATE, **res,
+            "speedup": round(res["zero"]["seconds"] / res["warm"]["seconds"], 3)}
 
 
 def main():
@@ -985,6 +1018,8 @@ def main():
     ap.add_argument("--fno-lr", type=float, default=2e-3)
     ap.add_argument("--fno-save", default=None)
     ap.add_argument("--fno-verbose", action="store_true")
+    ap.add_argument("--fno-headline", action="store_true",
+                    help="with --fno: also apply the trained network to the headline particle (x=20, L=64)")
     args = ap.parse_args()
     if args.large:
         run_large(args)
