@@ -270,20 +270,27 @@ def test_mixed_form_recovers_where_a_warm_complex128_restart_stagnates():
                      wl_0=1.0, m_m=1.0, workers=1)
     sc.DiscreteDipoles.verbose = False
     out = {}
-    for prec in (None, "mixed"):
+    for prec, tol in ((None, 1e-5), ("mixed", 1e-5), (None, 1e-10)):
         t = sc.Target("gre2", g["lattice_n"], g["lattice_lf"] * wl, g["grid"] * wl, g["is_in"], [mp] * 3)
         d = sc.DiscreteDipoles(t, sc.IncidentField(wl, 1.0, so3_euler(32, 308)))
-        d.tol, d.itermax, d.precision = 1e-5, 500, prec
+        d.tol, d.itermax, d.precision = tol, 800, prec
         d.set_interaction_matrix()
         d.solve_matrix_equation()
-        assert d.converge and d.err_fin < 1e-5, (prec, d.iter_fin, d.err_fin)
-        out[prec] = (d.iter_fin, d.observables())
-    assert out["mixed"][0] <= 120
-    o64, om = out[None][1], out["mixed"][1]
-    for cols in ((1,), (2, 3), (4, 5), (10, 11)):
-        a = om[:, cols[0]] + (1j * om[:, cols[1]] if len(cols) > 1 else 0)
-        b = o64[:, cols[0]] + (1j * o64[:, cols[1]] if len(cols) > 1 else 0)
-        assert np.max(np.abs(a - b)) / np.max(np.abs(b)) < 1e-3, cols
+        assert d.converge and d.err_fin < tol, (prec, d.iter_fin, d.err_fin)
+        out[(prec, tol)] = (d.iter_fin, d.observables())
+    assert out[("mixed", 1e-5)][0] <= 120
+    o64, om, oc = out[(None, 1e-5)][1], out[("mixed", 1e-5)][1], out[(None, 1e-10)][1]
+
+    def err(o, r, cols):
+        a = o[:, cols[0]] + (1j * o[:, cols[1]] if len(cols) > 1 else 0)
+        b = r[:, cols[0]] + (1j * r[:, cols[1]] if len(cols) > 1 else 0)
+        return np.max(np.abs(a - b)) / np.max(np.abs(b))
+    # C_ext and S_fw within 1e-4 of the complex128 path; S_bk (the most
+    # rounding-sensitive amplitude) as close to the converged solution as the
+    # complex128 path at the same tolerance is (within 3x, or 1e-4)
+    for cols in ((1,), (2, 3), (4, 5)):
+        assert err(om, o64, cols) < 1e-4, cols
+    assert err(om, oc, (10, 11)) < max(3 * err(o64, oc, (10, 11)), 1e-4)
 
 
 def test_mixed_form_converges_where_fp32_krylov_diverges(mods):
