@@ -131,18 +131,22 @@ class WarmStartFNO:
                                                 1 if train else 0, ptr(work), work.numel(),
                                                 stream_ptr(self.device)), "bdda_fno_forward")
 
-    # samples (orientations) per call: activations of at most max_rows lattice rows
+    # samples (orientations) per call: activations of at most max_rows lattice
+    # rows (~3 KB of workspace per row); inference takes larger calls, since
+    # its launches are few per call and the solve has not allocated yet
     max_rows = 4_000_000
+    max_rows_infer = 16_000_000
 
-    def _chunks(self, n, L):
-        per = max(1, min(L, self.max_rows // int(np.prod([int(v) for v in n]))))
+    def _chunks(self, n, L, rows=None):
+        rows = self.max_rows if rows is None else rows
+        per = max(1, min(L, rows // int(np.prod([int(v) for v in n]))))
         return [(c, min(L, c + per)) for c in range(0, L, per)]
 
     def predict(self, n, occ, diag, B, eps_r) -> torch.Tensor:
         """X0 = J + scale * FNO, complex128 (3 n_occ, L)."""
         L = int(B.shape[1])
         X0 = torch.empty_like(B)
-        for c0, c1 in self._chunks(n, L):
+        for c0, c1 in self._chunks(n, L, self.max_rows_infer):
             Bc = B[:, c0:c1].contiguous()
             work, scale = self.features(n, occ, diag, Bc, eps_r)
             self.forward(work, c1 - c0, n)
