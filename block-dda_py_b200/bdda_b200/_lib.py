@@ -48,6 +48,7 @@ PROTOTYPES = {
     "bdda_batch_workspace_bytes": (_sz, [_vp, _i, _i, _i, _i]),
     "bdda_mixed_workspace_bytes": (_sz, [_vp, _i, _i]),
     "bdda_tune_mixed": (_i, [_d, _d, _d]),
+    "bdda_tune_solver_graphs": (_i, [_i]),
     "bdda_tune_mixed_get": (_i, [_pd, _pd, _pd]),
     "bdda_fno_param_count": (_sz, [_vp]),
     "bdda_fno_offset": (_sz, [_vp, _i, _i]),

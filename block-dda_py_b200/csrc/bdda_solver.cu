@@ -5,8 +5,14 @@
 // xi, tau) lives in device memory.  Once per iteration a 16-byte status
 // (relative residual, breakdown flag) is read back to decide termination,
 // exactly where the reference tests ``err < tol`` (bl_krylov.py:110,181).
+// For small problems, where that read-back and the launches would dominate,
+// the plain solves instead capture one iteration as the body of a CUDA graph
+// "while" node: a one-thread kernel at the test point records the residual and
+// sets the loop condition on the device, so the whole solve is one graph
+// launch and one read-back.
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <type_traits>
 #include <utility>
 
@@ -19,8 +25,15 @@
 namespace bdda {
 
 struct Layout {
-  size_t field, vec[8], diag, jpre, partial, small, state, total;
+  size_t field, vec[8], diag, jpre, partial, small, state, hist, total;
 };
+
+// Residual history slots of the graph-driven loop (longer solves run the
+// host-driven loop), and the largest product work (padded grid points x L)
+// for which it is used: above it an iteration is long enough that the launches
+// and the read-back do not matter.
+constexpr int kGraphHistCap = 4096;
+constexpr double kGraphMaxWork = 64.0 * 1024 * 1024;
 
 constexpr int kVecs = 8;
 
@@ -38,6 +51,7 @@ static Layout layout(const bdda_plan* p, int prec, int L, int n_occ) {
   o.partial = off; off = al(off + (size_t)kRedBlocks * 2 * kMaxL * kMaxL * sizeof(double2));
   o.small = off; off = al(off + (size_t)kSmallMats * kMaxL * kMaxL * sizeof(double2) + 64 * sizeof(int));
   o.state = off; off = al(off + sizeof(SolverState));
+  o.hist = off; off = al(off + kGraphHistCap * sizeof(double));
   o.total = off;
   return o;
 }
@@ -233,6 +247,7 @@ struct Ctx {
   T* xbest = nullptr;      // mixed form: X at the smallest residual so far (or null)
   double best = INFINITY;  // that residual
   bool replaced = false;   // a residual replacement has happened
+  double* hist_dev = nullptr;   // graph-driven loop: per-iteration residuals (kGraphHistCap)
   bool watch = false;      // apply the divergence test to complex128 products too
 };
 
@@ -492,6 +507,199 @@ static int cocg_core(Ctx<T>& c, bool has_x0, double tol, int itermax, int* iter_
   return BDDA_NOT_CONVERGED;
 }
 
+// ---- graph-driven iteration loop ---------------------------------------------------
+// The test point of one iteration on the device: record the residual, count
+// the iteration, and keep looping while err >= tol, no breakdown or
+// non-finite value, and iterations remain.  The loop condition is the graph's
+// while-node handle; the counter bounds the loop by itermax whatever happens.
+__global__ void loop_check_kernel(SolverState* st, double tol, int itermax, double* hist,
+                                  cudaGraphConditionalHandle h) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const int k = st->iter;
+  const double err = st->err;
+  if (k < kGraphHistCap) hist[k] = err;
+  st->iter = k + 1;
+  const bool go = st->bad == 0 && !(err < tol) && k + 1 < itermax;
+  cudaGraphSetConditional(h, go ? 1u : 0u);
+}
+
+// Non-blocking stream per device for capturing the loop bodies (the caller's
+// stream may be the legacy default stream, which cannot be captured).
+static cudaStream_t capture_stream() {
+  static std::mutex mu;
+  static cudaStream_t streams[64] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+  std::lock_guard<std::mutex> lk(mu);
+  if (!streams[dev] && cudaStreamCreateWithFlags(&streams[dev], cudaStreamNonBlocking) != cudaSuccess)
+    streams[dev] = nullptr;
+  return streams[dev];
+}
+
+// Graph-driven loop: one while node whose body is `body(cc, h)` captured on a
+// private stream (cc = c with that stream), then one launch on c.stream and
+// one read-back.  Returns BDDA_OK / BREAKDOWN / NOT_CONVERGED like the
+// host-driven cores; any failure while building the graph returns
+// BDDA_CUDA_ERROR before anything ran (the caller then runs the host loop).
+template <typename T, typename Body>
+static int graph_loop(Ctx<T>& c, double tol, int itermax, int* iter_fin, double* err_fin, double* hist,
+                      Body body) {
+  cudaStream_t cs = capture_stream();
+  if (!cs) return BDDA_CUDA_ERROR;
+  cudaGraph_t g = nullptr;
+  cudaGraphExec_t ex = nullptr;
+  cudaGraphConditionalHandle h;
+  int status = BDDA_CUDA_ERROR;
+  long long n0 = 0, nbody = 0;
+  do {
+    if (cudaGraphCreate(&g, 0) != cudaSuccess) break;
+    if (cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault) != cudaSuccess) break;
+    cudaGraphNodeParams np = {cudaGraphNodeTypeConditional};
+    np.conditional.handle = h;
+    np.conditional.type = cudaGraphCondTypeWhile;
+    np.conditional.size = 1;
+    cudaGraphNode_t node;
+    if (cudaGraphAddNode(&node, g, nullptr, 0, &np) != cudaSuccess) break;
+    cudaGraph_t bodyg = np.conditional.phGraph_out[0];
+    Ctx<T> cc = c;
+    cc.stream = cs;
+    if (cudaStreamBeginCaptureToGraph(cs, bodyg, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed) != cudaSuccess)
+      break;
+    n0 = bdda_launch_count();
+    const int sb = body(cc, h);
+    cudaGraph_t captured = nullptr;
+    const cudaError_t ec = cudaStreamEndCapture(cs, &captured);
+    nbody = bdda_launch_count() - n0;
+    if (sb != BDDA_OK || ec != cudaSuccess) break;
+    if (cudaGraphInstantiate(&ex, g, 0) != cudaSuccess) break;
+    status = BDDA_OK;
+  } while (false);
+  if (status != BDDA_OK) {
+    cudaGetLastError();
+    if (ex) cudaGraphExecDestroy(ex);
+    if (g) cudaGraphDestroy(g);
+    return BDDA_CUDA_ERROR;
+  }
+  const cudaError_t el = cudaGraphLaunch(ex, c.stream);
+  SolverState hs;
+  const cudaError_t ec = el == cudaSuccess ? cudaMemcpyAsync(&hs, c.st, sizeof(hs), cudaMemcpyDeviceToHost, c.stream)
+                                           : el;
+  const cudaError_t es = ec == cudaSuccess ? cudaStreamSynchronize(c.stream) : ec;
+  cudaGraphExecDestroy(ex);
+  cudaGraphDestroy(g);
+  if (es != cudaSuccess) return BDDA_CUDA_ERROR;
+  const int ran = hs.iter < 1 ? 1 : (hs.iter > itermax ? itermax : hs.iter);
+  count_launch((int)(nbody * (ran - 1)));   // the body was counted once, at capture
+  if (hist) {
+    const int nh = ran < kGraphHistCap ? ran : kGraphHistCap;
+    BDDA_CUDA_TRY(cudaMemcpy(hist, c.hist_dev, nh * sizeof(double), cudaMemcpyDeviceToHost));
+  }
+  if (hs.bad == 1) return BDDA_BREAKDOWN;
+  *iter_fin = ran - 1;
+  *err_fin = hs.err;
+  if (hs.bad == 2) return BDDA_NOT_CONVERGED;
+  return hs.err < tol ? BDDA_OK : BDDA_NOT_CONVERGED;
+}
+
+// Block-BiCGSTAB with the graph-driven loop (plain forms, no complex64 products
+// inside complex128 vectors).  Same kernels and order as bicgstab_core.
+template <typename T>
+static int bicgstab_graph(Ctx<T>& c, bool has_x0, double tol, int itermax, int* iter_fin, double* err_fin,
+                          double* hist) {
+  T *X = c.vec[0], *R = c.vec[1], *P = c.vec[2], *R0 = c.vec[3], *V = c.vec[4], *Tt = c.vec[5],
+    *Z = c.vec[6], *Bj = c.vec[7];
+  const int L = c.L;
+  double* dot_partial = reinterpret_cast<double*>(c.partial) + 2 * (size_t)kMaxL * kMaxL * kRedBlocks;
+  TRY(upd<T>(c, R, Bj, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, true));
+  norm_kernel<<<1, 256, 0, c.stream>>>(reinterpret_cast<double*>(c.partial), kRedBlocks, c.st, 1);
+  count_launch();
+  BDDA_CUDA_TRY(cudaGetLastError());
+  if (has_x0) {
+    TRY(mvp_exact<T>(c, X, V));
+    TRY(upd<T>(c, R, Bj, nullptr, V, c.sp.r, nullptr, nullptr, nullptr, nullptr, false));
+  }
+  TRY(upd<T>(c, P, R, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, false));
+  TRY(upd<T>(c, R0, R, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, false));
+  *iter_fin = 0;
+  *err_fin = INFINITY;
+  return graph_loop<T>(c, tol, itermax, iter_fin, err_fin, hist, [&](Ctx<T>& cc, cudaGraphConditionalHandle h) -> int {
+    TRY(mvp<T>(cc, P, V));
+    TRY(gram2<T>(cc, true, R0, V, R, cc.sp.g2));
+    bicg_alpha_kernel<<<1, 256, cc.sm2, cc.stream>>>(cc.sp, L, cc.st);
+    count_launch();
+    TRY(upd<T>(cc, Tt, R, nullptr, nullptr, nullptr, V, nullptr, nullptr, cc.sp.negalpha, false));
+    TRY(mvp<T>(cc, Tt, Z));
+    TRY(gram2<T>(cc, true, R0, Z, nullptr, cc.sp.g2));
+    DotArgs d;
+    d.n = cc.n * L; d.A = Z; d.B = Tt; d.partial = dot_partial;
+    TRY(dots<T>(d, cc.stream));
+    bicg_zeta_beta_kernel<<<1, 256, cc.sm2, cc.stream>>>(cc.sp, L, dot_partial, kRedBlocks, cc.st);
+    count_launch();
+    TRY(upd<T>(cc, X, X, nullptr, Tt, &cc.st->zeta, P, nullptr, nullptr, cc.sp.alpha, false));
+    TRY(upd<T>(cc, R, Tt, nullptr, Z, &cc.st->negzeta, nullptr, nullptr, nullptr, nullptr, true));
+    norm_kernel<<<1, 256, 0, cc.stream>>>(reinterpret_cast<double*>(cc.partial), kRedBlocks, cc.st, 0);
+    loop_check_kernel<<<1, 32, 0, cc.stream>>>(cc.st, tol, itermax, cc.hist_dev, h);
+    count_launch(2);
+    TRY(upd<T>(cc, P, R, nullptr, nullptr, nullptr, P, V, &cc.st->negzeta, cc.sp.beta, false));
+    return cudaGetLastError() == cudaSuccess ? BDDA_OK : BDDA_CUDA_ERROR;
+  });
+}
+
+// Block-COCG-rq with the graph-driven loop.  The host loop swaps the roles of
+// two QR buffers every iteration; a captured body has fixed buffers, so the
+// new Q is copied into place instead (one vector copy per iteration, small at
+// the sizes this loop runs).
+template <typename T>
+static int cocg_graph(Ctx<T>& c, bool has_x0, double tol, int itermax, int* iter_fin, double* err_fin,
+                      double* hist) {
+  T *X = c.vec[0], *S = c.vec[4], *AS = c.vec[5], *W = c.vec[6], *Bj = c.vec[7];
+  T *Q = c.vec[1], *Q2 = c.vec[2], *Q3 = c.vec[3];
+  const int L = c.L;
+  TRY(upd<T>(c, W, Bj, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, true));
+  norm_kernel<<<1, 256, 0, c.stream>>>(reinterpret_cast<double*>(c.partial), kRedBlocks, c.st, 1);
+  count_launch();
+  BDDA_CUDA_TRY(cudaGetLastError());
+  if (has_x0) {
+    TRY(mvp_exact<T>(c, X, AS));
+    TRY(upd<T>(c, W, Bj, nullptr, AS, c.sp.r, nullptr, nullptr, nullptr, nullptr, false));
+  }
+  T* q = nullptr;
+  TRY(cholqr3<T>(c, W, Q2, Q3, &q));   // Q in Q2
+  BDDA_CUDA_TRY(cudaMemcpyAsync(Q, Q2, (size_t)c.n * L * sizeof(T), cudaMemcpyDeviceToDevice, c.stream));
+  cocg_xi_kernel<<<1, 256, c.sm3, c.stream>>>(c.sp, L, c.st, 1);
+  count_launch();
+  BDDA_CUDA_TRY(cudaGetLastError());
+  TRY(upd<T>(c, S, Q, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, false));
+  TRY(gram2<T>(c, false, Q, Q, nullptr, c.sp.qq));
+  *iter_fin = 0;
+  *err_fin = INFINITY;
+  return graph_loop<T>(c, tol, itermax, iter_fin, err_fin, hist, [&](Ctx<T>& cc, cudaGraphConditionalHandle h) -> int {
+    TRY(mvp<T>(cc, S, AS));
+    TRY(gram2<T>(cc, false, S, AS, nullptr, cc.sp.g2));
+    cocg_alpha_kernel<<<1, 256, cc.sm3, cc.stream>>>(cc.sp, L, cc.st);
+    count_launch();
+    TRY(upd<T>(cc, X, X, nullptr, nullptr, nullptr, S, nullptr, nullptr, cc.sp.alphaxi, false));
+    TRY(upd<T>(cc, W, Q, nullptr, nullptr, nullptr, AS, nullptr, nullptr, cc.sp.negalpha, false));
+    T* qn = nullptr;
+    TRY(cholqr3<T>(cc, W, Q2, Q3, &qn));   // Qnew in Q2, tau in sp.tau
+    cocg_xi_kernel<<<1, 256, cc.sm3, cc.stream>>>(cc.sp, L, cc.st, 0);
+    loop_check_kernel<<<1, 32, 0, cc.stream>>>(cc.st, tol, itermax, cc.hist_dev, h);
+    count_launch(2);
+    TRY(gram2<T>(cc, false, Q2, Q2, nullptr, cc.sp.g2));
+    cocg_beta_kernel<<<1, 256, cc.sm3, cc.stream>>>(cc.sp, L, cc.st);
+    count_launch();
+    TRY(upd<T>(cc, S, Q2, nullptr, nullptr, nullptr, S, nullptr, nullptr, cc.sp.beta, false));
+    if (cudaMemcpyAsync(Q, Q2, (size_t)cc.n * L * sizeof(T), cudaMemcpyDeviceToDevice, cc.stream) != cudaSuccess)
+      return BDDA_CUDA_ERROR;
+    return cudaGetLastError() == cudaSuccess ? BDDA_OK : BDDA_CUDA_ERROR;
+  });
+}
+
+// The host-driven loops are used when the graph-driven one is off
+// (bdda_tune_solver_graphs), the problem is large, the history would not fit,
+// or profiling records per-pass events.
+static int g_solver_graphs = 1;
+
 __global__ void constants_kernel(SmallPtrs s) {
   if (threadIdx.x == 0) s.r[0] = make_double2(-1.0, 0.0);
 }
@@ -548,6 +756,7 @@ static int run_solver(int solver, const bdda_plan* p, int L, int n_occ, const vo
   c.partial = reinterpret_cast<double2*>(w + o.partial);
   c.sp = small_ptrs(w + o.small);
   c.st = reinterpret_cast<SolverState*>(w + o.state);
+  c.hist_dev = reinterpret_cast<double*>(w + o.hist);
   c.stream = st;
   c.sm2 = (size_t)2 * L * L * sizeof(double2);
   c.sm3 = (size_t)3 * L * L * sizeof(double2);
@@ -574,9 +783,26 @@ static int run_solver(int solver, const bdda_plan* p, int L, int n_occ, const vo
   } else {
     BDDA_CUDA_TRY(cudaMemsetAsync(c.vec[0], 0, (size_t)c.n * L * sizeof(T), st));
   }
-  const int status = solver == BDDA_COCG_RQ
-                         ? cocg_core<T>(c, X0 != nullptr, tol, itermax, iter_fin, err_fin, hist)
-                         : bicgstab_core<T>(c, X0 != nullptr, tol, itermax, iter_fin, err_fin, hist);
+  const bool graph = g_solver_graphs && !profiling() && itermax <= kGraphHistCap &&
+                     (double)grid_points(p) * L <= kGraphMaxWork;
+  int status = BDDA_CUDA_ERROR;
+  if (graph) {
+    status = solver == BDDA_COCG_RQ ? cocg_graph<T>(c, X0 != nullptr, tol, itermax, iter_fin, err_fin, hist)
+                                    : bicgstab_graph<T>(c, X0 != nullptr, tol, itermax, iter_fin, err_fin, hist);
+  }
+  if (status == BDDA_CUDA_ERROR && graph) {   // the graph could not be built: start over on the host loop
+    BDDA_CUDA_TRY(cudaMemsetAsync(c.st, 0, sizeof(SolverState), st));
+    if (X0) {
+      convert_in_kernel<T><<<kRedBlocks, 256, 0, st>>>(X0, c.vec[0], c.n * L);
+      count_launch();
+      BDDA_CUDA_TRY(cudaGetLastError());
+    } else {
+      BDDA_CUDA_TRY(cudaMemsetAsync(c.vec[0], 0, (size_t)c.n * L * sizeof(T), st));
+    }
+  }
+  if (!graph || status == BDDA_CUDA_ERROR)
+    status = solver == BDDA_COCG_RQ ? cocg_core<T>(c, X0 != nullptr, tol, itermax, iter_fin, err_fin, hist)
+                                    : bicgstab_core<T>(c, X0 != nullptr, tol, itermax, iter_fin, err_fin, hist);
   if (status == BDDA_OK || status == BDDA_NOT_CONVERGED) {
     if (phys) {
       TRY(dda_epilogue<T>(*phys, c.vec[0], Xout, status == BDDA_OK, st));
@@ -1112,6 +1338,12 @@ int bdda_refine_solve(const bdda_plan* p, int solver, int L, int n_occ, const vo
                     static_cast<const double2*>(B), static_cast<const double2*>(X0), tol, itermax, inner_tol,
                     max_outer, static_cast<double2*>(X), iter_fin, err_fin, history, work, work_bytes,
                     (cudaStream_t)stream);
+}
+
+int bdda_tune_solver_graphs(int on) {
+  if (on != 0 && on != 1) return BDDA_BAD_ARG;
+  g_solver_graphs = on;
+  return BDDA_OK;
 }
 
 int bdda_tune_mixed(double replace_drop, double switch_ratio, double diverge_factor) {

@@ -15,7 +15,7 @@ struct SolverState {
   double bnorm;
   double err;
   int bad;      // 1: zero pivot (singular small system), 2: non-finite values
-  int pad;
+  int iter;     // iterations done (the graph-driven loop's counter)
 };
 
 // ---- one-CTA step kernels -------------------------------------------------------

@@ -254,6 +254,13 @@ size_t bdda_mixed_workspace_bytes(const bdda_plan* plan, int L, int n_occ);
  * (0, 1), default 0.1; switch_ratio >= 0, default 0 (complex64 products to
  * the end); diverge_factor > 1, default 10: the recursion counts as
  * diverged once its residual exceeds its smallest value so far by this. */
+/* Small one-problem solves (padded grid points x L <= 64 Mi, itermax <= 4096,
+ * plain complex128 / complex64 forms) run their iterations as a CUDA graph
+ * "while" node: one iteration is captured as the body and the loop condition
+ * is set on the device at the residual test, so a solve is one graph launch
+ * and one read-back instead of ~20 launches and a synchronisation per
+ * iteration.  on = 0 uses the host-driven loop everywhere (process-wide). */
+int bdda_tune_solver_graphs(int on);
 int bdda_tune_mixed(double replace_drop, double switch_ratio, double diverge_factor);
 int bdda_tune_mixed_get(double* replace_drop, double* switch_ratio, double* diverge_factor);
 int bdda_mixed_solve(const bdda_plan* plan, int solver, int L, int n_occ, const void* ghat_c128,

@@ -318,3 +318,55 @@ def test_mixed_form_converges_where_fp32_krylov_diverges(mods):
     # against the converged solution the mixed form is as accurate as complex128 at the same tolerance
     for key in ("C_ext", "S_fw_theta", "S_fw_phi", "S_bk"):
         assert rel(om[key], oc[key]) < max(3 * rel(o64[key], oc[key]), 1e-5), key
+
+
+@pytest.mark.parametrize("solver", ["bicgstab", "cocg"])
+@pytest.mark.parametrize("prec", [None, "c64"])
+def test_graph_driven_loop_matches_the_host_loop(mods, solver, prec):
+    """Small solves run their iterations as a CUDA graph while node (the loop
+    condition set on the device at the residual test); the same solve with the
+    host-driven loop gives the same iterates, residual history and count."""
+    from bdda_b200 import _lib
+    mf, bk = mods
+    g = load_golden("solver_small")
+    til = mf.fft_init(g["n"], 3, float(g["lf"]), float(g["k"]))
+    lib = _lib.load()
+    res = {}
+    try:
+        for on in (1, 0):
+            assert lib.bdda_tune_solver_graphs(on) == 0
+            h = []
+            n0 = lib.bdda_launch_count()
+            X, it, err = solver_fn(bk, solver)(g["n"], 3, g["address"], til, g["diag_A"], g["B"], 1e-9, 300,
+                                               precision=prec, history=h)
+            res[on] = (X, it, err, h, lib.bdda_launch_count() - n0)
+    finally:
+        lib.bdda_tune_solver_graphs(1)
+    assert res[1][1] == res[0][1] and res[1][1] > 5
+    assert res[1][2] == res[0][2]
+    assert res[1][3] == res[0][3]
+    assert np.array_equal(res[1][0], res[0][0])
+    # the launch counter counts the kernels the graph ran, as the host loop does
+    # (COCG's graph adds no kernel: it copies the new Q in place of the swap)
+    assert abs(res[1][4] - res[0][4]) <= 4
+
+
+def test_graph_driven_loop_stops_at_itermax(mods):
+    """A solve that cannot converge stops after exactly itermax iterations in
+    the graph-driven loop, with the host loop's count and residual."""
+    from bdda_b200 import _lib
+    mf, bk = mods
+    g = load_golden("solver_small")
+    til = mf.fft_init(g["n"], 3, float(g["lf"]), float(g["k"]))
+    lib = _lib.load()
+    out = {}
+    try:
+        for on in (1, 0):
+            lib.bdda_tune_solver_graphs(on)
+            h = []
+            X, it, err = bk.bl_bicgstab_jacobi_mvp_fft(g["n"], 3, g["address"], til, g["diag_A"], g["B"], 1e-30, 7,
+                                                       history=h)
+            out[on] = (it, err, len(h))
+    finally:
+        lib.bdda_tune_solver_graphs(1)
+    assert out[1] == out[0] == (6, out[0][1], 7)
