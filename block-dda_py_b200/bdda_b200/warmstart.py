@@ -209,9 +209,17 @@ class WarmStartFNO:
         return losses
 
     # ---- warm start with the fallback rule ----
-    def warm_start(self, n, occ, green, diag, B, eps_r):
-        """(X0 or None, columns that fell back): a column whose predicted initial
-        residual ||M^-1 (B - A X0)|| exceeds ||M^-1 B|| starts from zero."""
+    def warm_start(self, n, occ, green, diag, B, eps_r, mode="fallback"):
+        """(X0 or None, columns that fell back).
+
+        mode "fallback": a column whose predicted initial residual
+        ||M^-1 (B - A X0)|| exceeds ||M^-1 B|| starts from zero.  mode
+        "project": X0 = P G with P the L predicted columns and G (L x L) the
+        least-squares fit min ||M^-1 B - (M^-1 A P) G||_F, from the same one
+        product; its residual is at most the zero start's (G = 0 is a
+        candidate), so no column falls back.  Either way the solver still
+        runs to its tolerance and judges the result.
+        """
         L = int(B.shape[1])
         if not self.supports(n):
             return None, L
@@ -224,6 +232,12 @@ class WarmStartFNO:
                                       ptr(diag), ptr(jpre), ptr(X0), ptr(AX), ptr(work),
                                       stream_ptr(self.device)), "bdda_block_mvp")
         Bj = B * jpre[:, None]
+        if mode == "project":
+            G = AX.conj().T @ AX                      # L x L normal equations (complex128)
+            rhs = AX.conj().T @ Bj
+            ridge = 1e-12 * torch.diagonal(G).real.mean().clamp_min(1e-300)
+            coef = torch.linalg.solve(G + ridge * torch.eye(L, dtype=G.dtype, device=G.device), rhs)
+            return X0 @ coef, 0
         r = torch.linalg.vector_norm(Bj - AX, dim=0)
         b = torch.linalg.vector_norm(Bj, dim=0)
         bad = ~(r <= b)

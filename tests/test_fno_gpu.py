@@ -134,3 +134,16 @@ def test_trained_warm_start_gains_over_zero_start():
         it_warm += i1 + 1
     assert max(r0) <= 1.0 + 1e-9 and np.mean(r0) < 0.95
     assert it_warm <= it_zero + 2
+    # the projected start (least-squares fit over the predicted columns) starts
+    # no higher than the per-column fallback, and converges to the same tolerance
+    for d, r_fb in zip(held, r0):
+        Xp, nfb = model.warm_start(d["n"], d["occ"], d["green"], d["diag"], d["B"], d["eps_r"], mode="project")
+        assert nfb == 0
+        Bj = d["B"] / d["diag"][:, None]
+        AX = bk._block_mvp(d["n"], 3, d["green"], bk._build_scatter_index(d["occ"].address, 3), d["diag"], Xp,
+                           1.0 / d["diag"])
+        rp = float((torch.linalg.vector_norm(Bj - AX) / torch.linalg.vector_norm(Bj)).item())
+        assert rp <= r_fb + 1e-9
+        _, ip, ep = bk.bl_bicgstab_jacobi_mvp_fft(d["n"], 3, d["occ"], d["green"], d["diag"], d["B"], 1e-5, 400,
+                                                  X0=Xp)
+        assert ep < 1e-5
