@@ -72,6 +72,7 @@ PROTOTYPES = {
     "bdda_plan_radices": (_i, [_vp, _i, _pi, _pi]),
     "bdda_plan_table_bytes": (_sz, [_vp]),
     "bdda_plan_attach_tables": (_i, [_vp, _vp, _vp]),
+    "bdda_plan_wait_timeouts": (_i, [_vp, C.POINTER(C.c_uint), _vp]),
     "bdda_green_bytes": (_sz, [_vp, _i]),
     "bdda_green_build_workspace_bytes": (_sz, [_vp]),
     "bdda_green_build": (_i, [_vp, _d, _d, _vp, _vp, _vp]),

@@ -101,6 +101,13 @@ class Plan:
     def mvp_workspace_bytes(self, prec: int, L: int) -> int:
         return int(_lib.load().bdda_mvp_workspace_bytes(self._h, prec, int(L)))
 
+    def wait_timeouts(self) -> int:
+        """Bounded waits of this plan's pass kernels that ran out (0 in a correct run)."""
+        c = C.c_uint()
+        _lib.check(_lib.load().bdda_plan_wait_timeouts(self._h, C.byref(c), stream_ptr(self.device)),
+                   "bdda_plan_wait_timeouts")
+        return int(c.value)
+
     def __del__(self):
         h = getattr(self, "_h", None)
         if h is not None and _lib._lib is not None:

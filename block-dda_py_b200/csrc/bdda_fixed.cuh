@@ -11,6 +11,11 @@
 // slower).  bdda_fixed_*.cu instantiate the sequences the planner produces
 // for the workloads; fixed_find() in bdda_mvp.cu dispatches to them.
 #pragma once
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <mutex>
+
 #include "bdda_pencil.cuh"
 
 namespace bdda {
@@ -213,25 +218,133 @@ __device__ __forceinline__ void fixed_mid(const PassArgs& a, const Pen& c, T* sm
   }
 }
 
+// ---- the tile's first read by a bulk tensor copy (TMA) ------------------------------------
+// With TMA = 1 the pencil's source rows of the CTA's column tile come into the
+// shared tile by one or two cp.async.bulk.tensor copies, issued by one thread
+// before the constants are staged (all bytes in flight at once); the first
+// radix stage then reads shared memory instead of issuing its own global
+// loads.  The tensor map views the source field as (l, component, row, p1,
+// p0), the last three ordered by stride, so a box lands as rows of the
+// [row][3 LT] tile; rows at or past n_in and columns at or past L come back
+// as zeros (out-of-bounds fill), as gload returns them.  Two boxes of
+// box_rows rows start at rows 0 and M - box_rows (they may overlap by a row
+// or two, written twice with the same bytes) so that each starts on a
+// 128-byte boundary of the tile.  The copy completes on a transaction
+// barrier; the wait is bounded, and a CTA that gives up counts the event in
+// a.err, waits (bounded again) for its copy to land and returns.
+struct TmaTile {
+  int nbox, box_rows;
+  int dim_of[3];   // dimension 2 + d of the map holds (row, p1, p0)[dim_of[d]]
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity, int limit) {
+  for (int i = 0; i < limit; ++i) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+constexpr int kTmaWaitLimit = 1 << 22;   // try_wait rounds: far beyond any copy's latency, but finite
+
+template <typename T, int KIND, int LT>
+__device__ __forceinline__ void tma_issue(const PassArgs& a, const CUtensorMap* tm, const TmaTile& tt,
+                                          unsigned char* smraw, int M, int64_t bid) {
+  constexpr int E = sizeof(T) / 8;   // 8-byte elements per complex value
+  T* sm = pencil_tile<T, LT>(smraw, M);
+  const uint32_t bar = smem_u32(pencil_barrier<T, KIND, LT>(smraw, M));
+  const int tile = (int)(bid % a.ntile);
+  const int64_t p = bid / a.ntile;
+  const int64_t p0 = p / a.P1, p1 = p - p0 * a.P1;
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(bar) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+  const uint32_t bytes = (uint32_t)(tt.nbox * tt.box_rows * 3 * LT * (int)sizeof(T));
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes) : "memory");
+  for (int b = 0; b < tt.nbox; ++b) {
+    const int row0 = b == 0 ? 0 : M - tt.box_rows;
+    const int v[3] = {row0, (int)p1, (int)p0};
+    int c[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) c[d] = v[tt.dim_of[d]];
+    const uint32_t dst = smem_u32(sm + (size_t)row0 * 3 * LT);
+    asm volatile(
+        "cp.async.bulk.tensor.5d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5, "
+        "%6}], [%7];\n" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(tm)), "r"(tile * LT * E), "r"(0), "r"(c[0]), "r"(c[1]), "r"(c[2]), "r"(bar)
+        : "memory");
+  }
+}
+
+// First stage of a pass: reads the TMA-filled tile (from_tile) or global memory.
+template <class RS, int S, bool INV, int DST, int KIND, typename T, int LT, int NT, int PAIR, int TMA>
+__device__ __forceinline__ void first_stage(const PassArgs& a, const Pen& c, T* sm, const T* tw, bool from_tile) {
+  if constexpr (TMA) {
+    if (from_tile) {
+      fixed_stage<RS, S, INV, 0, DST, KIND, T, LT, NT, PAIR>(a, c, sm, tw);
+      return;
+    }
+  }
+  fixed_stage<RS, S, INV, 1, DST, KIND, T, LT, NT, PAIR>(a, c, sm, tw);
+}
+template <class RS, typename T, int LT, int NT, int PAIR, int TMA>
+__device__ __forceinline__ void first_mid(const PassArgs& a, const Pen& c, T* sm, const T* gs, bool from_tile) {
+  if constexpr (TMA) {
+    if (from_tile) {
+      fixed_mid<RS, 0, 1, T, LT, NT, PAIR>(a, c, sm, gs);
+      return;
+    }
+  }
+  fixed_mid<RS, 1, 1, T, LT, NT, PAIR>(a, c, sm, gs);
+}
+
 // NT: threads per CTA.  MINB: resident CTAs per SM the register allocation
 // must allow (the __launch_bounds__ minimum); 1 = no bound.  PAIR: column
-// pairs per job (complex64).  Kernels are compiled with several (NT, MINB,
-// PAIR) and the autotuner picks per pass.
-template <typename T, int KIND, int LT, int NT, int MINB, int R0, int R1, int R2, int R3, int PAIR>
-__global__ void __launch_bounds__(NT, MINB) fixed_pencil_kernel(const PassArgs a) {
+// pairs per job (complex64).  TMA: the first read of the tile is a bulk tensor
+// copy (dense sources only; make_tile_map).  Kernels are compiled with several
+// (NT, MINB, PAIR, TMA) and the autotuner picks per pass.
+template <typename T, int KIND, int LT, int NT, int MINB, int R0, int R1, int R2, int R3, int PAIR, int TMA>
+__global__ void __launch_bounds__(NT, MINB) fixed_pencil_kernel(const PassArgs a, const __grid_constant__ CUtensorMap tm,
+                                                                const TmaTile tt) {
   static_assert(!PAIR || (std::is_same<T, float2>::value && LT % 2 == 0), "column pairs are complex64, even LT");
   using RS = RadixSeq<R0, R1, R2, R3>;
   constexpr int N = RS::n;
-  extern __shared__ __align__(16) unsigned char smraw[];
+  extern __shared__ __align__(128) unsigned char smraw[];
+  // the bulk copy needs a 128-byte aligned destination; otherwise (not seen:
+  // dynamic shared memory starts on a wide boundary) the plain global reads
+  const bool from_tile = TMA && (smem_u32(pencil_tile<T, LT>(smraw, RS::M)) & 127) == 0;
+  if constexpr (TMA) {
+    if (from_tile && threadIdx.x == 0) tma_issue<T, KIND, LT>(a, &tm, tt, smraw, RS::M, blockIdx.x);
+  }
   T *tw, *sm, *gs;
   int32_t* cm;
   stage_constants<T, KIND, LT>(a, smraw, RS::M, &tw, &sm, &gs, &cm, blockIdx.x);
   const Pen c = pen_of_block<T>(a, cm, blockIdx.x);
+  if constexpr (TMA) {
+    if (from_tile) {
+      const uint32_t bar = smem_u32(pencil_barrier<T, KIND, LT>(smraw, RS::M));
+      const bool landed = mbar_wait_bounded(bar, 0, kTmaWaitLimit);
+      if (__syncthreads_or(!landed)) {   // the whole CTA leaves together
+        if (threadIdx.x == 0) {
+          if (a.err) atomicAdd(a.err, 1u);
+          mbar_wait_bounded(bar, 0, kTmaWaitLimit);   // the copy lands before the CTA's shared memory is released
+        }
+        return;
+      }
+    }
+  }
   if constexpr (KIND == K_FWD) {
     if constexpr (N == 1) {
-      fixed_stage<RS, 0, false, 1, 1, KIND, T, LT, NT, PAIR>(a, c, sm, tw);
+      first_stage<RS, 0, false, 1, KIND, T, LT, NT, PAIR, TMA>(a, c, sm, tw, from_tile);
     } else {
-      fixed_stage<RS, 0, false, 1, 0, KIND, T, LT, NT, PAIR>(a, c, sm, tw);
+      first_stage<RS, 0, false, 0, KIND, T, LT, NT, PAIR, TMA>(a, c, sm, tw, from_tile);
       __syncthreads();
       if constexpr (N >= 3) { fixed_stage<RS, 1, false, 0, 0, KIND, T, LT, NT, PAIR>(a, c, sm, tw); __syncthreads(); }
       if constexpr (N >= 4) { fixed_stage<RS, 2, false, 0, 0, KIND, T, LT, NT, PAIR>(a, c, sm, tw); __syncthreads(); }
@@ -239,9 +352,9 @@ __global__ void __launch_bounds__(NT, MINB) fixed_pencil_kernel(const PassArgs a
     }
   } else if constexpr (KIND == K_INV) {
     if constexpr (N == 1) {
-      fixed_stage<RS, 0, true, 1, 1, KIND, T, LT, NT, PAIR>(a, c, sm, tw);
+      first_stage<RS, 0, true, 1, KIND, T, LT, NT, PAIR, TMA>(a, c, sm, tw, from_tile);
     } else {
-      fixed_stage<RS, N - 1, true, 1, 0, KIND, T, LT, NT, PAIR>(a, c, sm, tw);
+      first_stage<RS, N - 1, true, 0, KIND, T, LT, NT, PAIR, TMA>(a, c, sm, tw, from_tile);
       __syncthreads();
       if constexpr (N >= 4) { fixed_stage<RS, 2, true, 0, 0, KIND, T, LT, NT, PAIR>(a, c, sm, tw); __syncthreads(); }
       if constexpr (N >= 3) { fixed_stage<RS, 1, true, 0, 0, KIND, T, LT, NT, PAIR>(a, c, sm, tw); __syncthreads(); }
@@ -251,9 +364,9 @@ __global__ void __launch_bounds__(NT, MINB) fixed_pencil_kernel(const PassArgs a
     cp_async_wait<0>();
     __syncthreads();
     if constexpr (N == 1) {
-      fixed_mid<RS, 1, 1, T, LT, NT, PAIR>(a, c, sm, gs);
+      first_mid<RS, T, LT, NT, PAIR, TMA>(a, c, sm, gs, from_tile);
     } else {
-      fixed_stage<RS, 0, false, 1, 0, KIND, T, LT, NT, PAIR>(a, c, sm, tw);
+      first_stage<RS, 0, false, 0, KIND, T, LT, NT, PAIR, TMA>(a, c, sm, tw, from_tile);
       __syncthreads();
       if constexpr (N >= 3) { fixed_stage<RS, 1, false, 0, 0, KIND, T, LT, NT, PAIR>(a, c, sm, tw); __syncthreads(); }
       if constexpr (N >= 4) { fixed_stage<RS, 2, false, 0, 0, KIND, T, LT, NT, PAIR>(a, c, sm, tw); __syncthreads(); }
@@ -266,7 +379,84 @@ __global__ void __launch_bounds__(NT, MINB) fixed_pencil_kernel(const PassArgs a
   }
 }
 
-template <typename T, int KIND, int LT, int MINB, int NT, int PAIR, int R0, int R1, int R2, int R3>
+// cuTensorMapEncodeTiled from the driver, looked up once through the runtime
+// (no link against the driver library).
+inline PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static std::once_flag once;
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  });
+  return fn;
+}
+
+// Rows of the one or two boxes that fill an M-row tile (box 1 starts at
+// M - box_rows, 128-byte aligned in the tile); false if M needs more.
+inline bool tile_boxes(int M, int row_bytes, int* nbox, int* box_rows) {
+  if (M < 1) return false;
+  if (M <= 256) {
+    *nbox = 1;
+    *box_rows = M;
+    return true;
+  }
+  int g = 1;   // rows per 128-byte granule of the tile
+  while ((g * row_bytes) % 128) ++g;
+  int br = (M + 1) / 2;
+  while ((M - br) % g) ++br;
+  if (br > 256 || M > 512) return false;
+  *nbox = 2;
+  *box_rows = br;
+  return true;
+}
+
+// Tensor map of the tile copies of a pass.  False when the pass cannot use
+// them: a gathered or evaluated source, a source pointer, column offset or
+// stride that is not a 16-byte multiple, or a tile of more than two boxes.
+template <typename T, int KIND, int LT>
+bool make_tile_map(const PassArgs& a, int64_t P0, int M, CUtensorMap* tm, TmaTile* tt) {
+  constexpr int E = sizeof(T) / 8;
+  const int64_t s = sizeof(T);
+  if ((KIND == K_FWD && a.cell_map) || a.green || !a.src) return false;
+  // x coordinates are multiples of LT * s bytes: they must be 16-byte multiples
+  if ((reinterpret_cast<uintptr_t>(a.src) & 15) || (LT * s) % 16 || (a.L * s) % 16) return false;
+  if (a.n_in < 1 || a.P1 < 1 || P0 < 1 || a.L < 1) return false;
+  const int64_t strides[3] = {a.src_row * s, a.src_p1 * s, a.src_p0 * s};
+  for (int64_t st : strides)
+    if (st <= 0 || st % 16 || st >= ((int64_t)1 << 40)) return false;
+  int nbox, box_rows;
+  if (!tile_boxes(M, 3 * LT * (int)s, &nbox, &box_rows)) return false;
+  auto enc = tensor_map_encoder();
+  if (!enc) return false;
+  // dimensions 2..4: (row, p1, p0) ordered by stride
+  int order[3] = {0, 1, 2};
+  for (int i = 0; i < 3; ++i)
+    for (int j = i + 1; j < 3; ++j)
+      if (strides[order[j]] < strides[order[i]]) std::swap(order[i], order[j]);
+  const int64_t ext[3] = {a.n_in, a.P1, P0};
+  const int box3[3] = {box_rows, 1, 1};
+  cuuint64_t gdim[5] = {(cuuint64_t)a.L * E, 3, 0, 0, 0};
+  cuuint64_t gstride[4] = {(cuuint64_t)(a.L * s), 0, 0, 0};
+  cuuint32_t box[5] = {(cuuint32_t)(LT * E), 3, 0, 0, 0};
+  cuuint32_t estr[5] = {1, 1, 1, 1, 1};
+  for (int d = 0; d < 3; ++d) {
+    gdim[2 + d] = (cuuint64_t)ext[order[d]];
+    gstride[1 + d] = (cuuint64_t)strides[order[d]];
+    box[2 + d] = (cuuint32_t)box3[order[d]];
+    tt->dim_of[d] = order[d];
+  }
+  tt->nbox = nbox;
+  tt->box_rows = box_rows;
+  const CUresult r = enc(tm, CU_TENSOR_MAP_DATA_TYPE_UINT64, 5, const_cast<void*>(a.src), gdim, gstride, box, estr,
+                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
+template <typename T, int KIND, int LT, int MINB, int NT, int PAIR, int R0, int R1, int R2, int R3, int TMA = 0>
 int fixed_launch(const PassArgs& a0, int64_t P0, cudaStream_t st) {
   static_assert(NT % 32 == 0 && NT <= 512 && MINB >= 1 && MINB < 16, "variant id encodes whole warps and MINB < 16");
   using RS = RadixSeq<R0, R1, R2, R3>;
@@ -274,14 +464,20 @@ int fixed_launch(const PassArgs& a0, int64_t P0, cudaStream_t st) {
   if (a.ax.M != RS::M) return BDDA_BAD_ARG;
   if (PAIR && (a.L % 2) != 0) return BDDA_BAD_ARG;
   a.ntile = (a.L + LT - 1) / LT;
-  auto kern = fixed_pencil_kernel<T, KIND, LT, NT, MINB, R0, R1, R2, R3, PAIR>;
+  CUtensorMap tm;
+  memset(&tm, 0, sizeof(tm));
+  TmaTile tt;
+  memset(&tt, 0, sizeof(tt));
+  if (TMA && !make_tile_map<T, KIND, LT>(a, P0, RS::M, &tm, &tt))   // not possible for this pass: the plain kernel
+    return fixed_launch<T, KIND, LT, MINB, NT, PAIR, R0, R1, R2, R3, 0>(a0, P0, st);
+  auto kern = fixed_pencil_kernel<T, KIND, LT, NT, MINB, R0, R1, R2, R3, PAIR, TMA>;
   const size_t smem = (size_t)pencil_smem_bytes<T>(RS::M, LT, KIND);
   if (smem > 227 * 1024) return BDDA_BAD_ARG;
   const int64_t nblk = P0 * a.P1 * a.ntile;
   if (nblk <= 0) return BDDA_OK;
   if (nblk > 0x7fffffff) return BDDA_BAD_ARG;
   BDDA_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  kern<<<(unsigned)nblk, NT, smem, st>>>(a);
+  kern<<<(unsigned)nblk, NT, smem, st>>>(a, tm, tt);
   BDDA_CUDA_TRY(cudaGetLastError());
   count_launch();
   return BDDA_OK;
@@ -299,5 +495,12 @@ int fixed_launch(const PassArgs& a0, int64_t P0, cudaStream_t st) {
 #define BDDA_FIXED_PAIR(PREC, KIND, LT, MINB, NT, R0, R1, R2, R3)                                 \
   { PREC, KIND, LT, MINB, 512 + MINB + 16 * ((NT) / 32), {R0, R1, R2, R3},                        \
     &fixed_launch<float2, KIND, LT, MINB, NT, 1, R0, R1, R2, R3>, 1 }
+// The same with the tile's first read by a bulk tensor copy: ids + 1024.
+#define BDDA_FIXED_TMA_NT(T, PREC, KIND, LT, MINB, NT, R0, R1, R2, R3)                          \
+  { PREC, KIND, LT, MINB, 1024 + MINB + 16 * ((NT) / 32), {R0, R1, R2, R3},                       \
+    &fixed_launch<T, KIND, LT, MINB, NT, 0, R0, R1, R2, R3, 1>, 0 }
+#define BDDA_FIXED_TMA_PAIR(PREC, KIND, LT, MINB, NT, R0, R1, R2, R3)                             \
+  { PREC, KIND, LT, MINB, 1024 + 512 + MINB + 16 * ((NT) / 32), {R0, R1, R2, R3},                 \
+    &fixed_launch<float2, KIND, LT, MINB, NT, 1, R0, R1, R2, R3, 1>, 1 }
 
 }  // namespace bdda

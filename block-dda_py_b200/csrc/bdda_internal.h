@@ -15,6 +15,7 @@ struct bdda_plan {
   size_t tw64_off[3];   // double2[M]: exp(-2 pi i k / M)
   size_t tw32_off[3];   // float2[M]: the same, rounded
   size_t rev_off[3];    // int32[M]: stored position -> frequency index
+  size_t err_off;       // uint32: bounded waits of the plan's kernels that gave up
   size_t table_bytes;
   std::vector<unsigned char> host_tables;
   void* dev_tables;
@@ -44,6 +45,10 @@ inline size_t cplx_bytes(int prec) { return prec == BDDA_C64 ? 8 : 16; }
 template <typename T>
 inline const T* table_ptr(const bdda_plan* p, size_t off) {
   return reinterpret_cast<const T*>(static_cast<const unsigned char*>(p->dev_tables) + off);
+}
+inline unsigned int* plan_err(const bdda_plan* p) {
+  return p->dev_tables ? reinterpret_cast<unsigned int*>(static_cast<unsigned char*>(p->dev_tables) + p->err_off)
+                       : nullptr;
 }
 
 // Residual replacement drop and divergence factor of the mixed-form

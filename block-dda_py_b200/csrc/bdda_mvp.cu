@@ -99,7 +99,7 @@ static int launch_lt(PassArgs a, int64_t P0, cudaStream_t st) {
 
 static int g_use_fixed = 1;   // specialised kernels on (bdda_tune_fixed)
 
-static constexpr int kFixedTables = 8;
+static constexpr int kFixedTables = 9;
 
 static const FixedKernel* fixed_table(int t, int* n) {
   switch (t) {
@@ -110,7 +110,8 @@ static const FixedKernel* fixed_table(int t, int* n) {
     case 4: return fixed_table_e(n);
     case 5: return fixed_table_f(n);
     case 6: return fixed_table_g(n);
-    default: return fixed_table_h(n);
+    case 7: return fixed_table_h(n);
+    default: return fixed_table_i(n);
   }
 }
 
@@ -200,6 +201,7 @@ void mvp_pass_args(const bdda_plan* plan, int L, const T* ghat, const int32_t* c
   b.L = L;
   b.C = C;
   b.scale = 1.0;
+  b.err = plan_err(plan);
   {  // Z: gather + forward z
     PassArgs& q = a[0];
     q = b;
@@ -547,7 +549,7 @@ int bdda_tune_set(int prec, int kind, size_t smem_budget, int threads) {
 
 int bdda_tune_pass(int prec, int kind, int M, int L, int lt, int variant) {
   if (prec < 0 || prec > 1 || kind < 0 || kind > 2 || M < 1 || L < 1 || L > kMaxL ||
-      (lt != 0 && lt != 2 && lt != 4 && lt != 8) || variant < -1 || variant > 1024)
+      (lt != 0 && lt != 2 && lt != 4 && lt != 8 && lt != 16) || variant < -1 || variant >= 2048)
     return BDDA_BAD_ARG;
   set_pass_tune({prec, kind, M, L, lt, variant});
   return BDDA_OK;
@@ -629,6 +631,7 @@ int bdda_plan_create(const int n[3], const int m[3], bdda_plan** out) {
     p->tw32_off[a] = off; off = align256(off + (size_t)M * sizeof(float2));
     p->rev_off[a] = off;  off = align256(off + (size_t)M * sizeof(int32_t));
   }
+  p->err_off = off; off = align256(off + sizeof(uint32_t));
   p->table_bytes = off;
   p->host_tables.assign(off, 0);
   for (int a = 0; a < 3; ++a) {
@@ -676,6 +679,15 @@ int bdda_plan_radices(const bdda_plan* p, int axis, int radices[12], int* nstage
 }
 
 size_t bdda_plan_table_bytes(const bdda_plan* p) { return p ? p->table_bytes : 0; }
+
+int bdda_plan_wait_timeouts(const bdda_plan* p, unsigned int* count, void* stream) {
+  if (!p || !count) return BDDA_BAD_ARG;
+  if (!p->dev_tables) return BDDA_NO_WORKSPACE;
+  cudaStream_t st = (cudaStream_t)stream;
+  BDDA_CUDA_TRY(cudaMemcpyAsync(count, plan_err(p), sizeof(unsigned int), cudaMemcpyDeviceToHost, st));
+  BDDA_CUDA_TRY(cudaStreamSynchronize(st));
+  return BDDA_OK;
+}
 
 int bdda_plan_attach_tables(bdda_plan* p, void* dev, void* stream) {
   if (!p || !dev || (reinterpret_cast<uintptr_t>(dev) & 15)) return BDDA_BAD_ARG;

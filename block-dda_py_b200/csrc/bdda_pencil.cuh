@@ -41,6 +41,7 @@ struct PassArgs {
   const void* ghat;
   int gN[3], gM[3];
   double lf, k;
+  unsigned int* err;    // bounded waits that gave up (the plan's counter; null: not counted)
 };
 
 struct Pen {
@@ -107,13 +108,17 @@ __device__ __forceinline__ void async_copy(void* dst, const void* src, int nbyte
 }
 
 __host__ __device__ __forceinline__ int align16(int x) { return (x + 15) & ~15; }
+__host__ __device__ __forceinline__ int align128(int x) { return (x + 127) & ~127; }
 
 template <typename T> constexpr int prec_of() { return std::is_same<T, double2>::value ? 0 : 1; }
 
+// Shared memory of one pencil CTA: twiddles, the [row][3 LT] tile (128-byte
+// aligned: a bulk tensor copy may fill it), the Green's pencil (X pass), the
+// occupancy-map rows and one 8-byte transaction barrier.
 template <typename T>
 __host__ __device__ __forceinline__ int pencil_smem_bytes(int M, int LT, int kind) {
-  return align16(M * (int)sizeof(T)) + align16(M * 3 * LT * (int)sizeof(T)) +
-         (kind == K_CONV ? align16(M * 6 * (int)sizeof(T)) : 0) + align16(M * 4);
+  return align128(M * (int)sizeof(T)) + align16(M * 3 * LT * (int)sizeof(T)) +
+         (kind == K_CONV ? align16(M * 6 * (int)sizeof(T)) : 0) + align16(M * 4) + 16;
 }
 
 // Pencil and tile of a CTA (one item per CTA).
@@ -133,9 +138,19 @@ __device__ __forceinline__ Pen pen_of_block(const PassArgs& a, const int32_t* cm
 // Shared-memory carve-up and the asynchronous staging of the twiddles (and,
 // for the X pass, the Green's pencil).  Returns after the twiddles landed.
 template <typename T, int KIND, int LT>
+__device__ __forceinline__ unsigned char* pencil_barrier(unsigned char* smraw, int M) {
+  return smraw + align128(M * (int)sizeof(T)) + align16(M * 3 * LT * (int)sizeof(T)) +
+         (KIND == K_CONV ? align16(M * 6 * (int)sizeof(T)) : 0) + align16(M * 4);
+}
+template <typename T, int LT>
+__device__ __forceinline__ T* pencil_tile(unsigned char* smraw, int M) {
+  return reinterpret_cast<T*>(smraw + align128(M * (int)sizeof(T)));
+}
+
+template <typename T, int KIND, int LT>
 __device__ __forceinline__ void stage_constants(const PassArgs& a, unsigned char* smraw, int M, T** tw, T** sm,
                                                 T** gs, int32_t** cm, int64_t bid) {
-  const int o_sm = align16(M * (int)sizeof(T));
+  const int o_sm = align128(M * (int)sizeof(T));
   const int o_gs = o_sm + align16(M * 3 * LT * (int)sizeof(T));
   const int o_cm = o_gs + (KIND == K_CONV ? align16(M * 6 * (int)sizeof(T)) : 0);
   *tw = reinterpret_cast<T*>(smraw);
@@ -438,6 +453,7 @@ const FixedKernel* fixed_table_e(int* n);
 const FixedKernel* fixed_table_f(int* n);
 const FixedKernel* fixed_table_g(int* n);
 const FixedKernel* fixed_table_h(int* n);
+const FixedKernel* fixed_table_i(int* n);
 
 
 }  // namespace bdda

@@ -81,6 +81,11 @@ int bdda_plan_radices(const bdda_plan* plan, int axis, int radices[12], int* nst
  * bdda_plan_table_bytes(); the plan uploads into it and keeps the pointer. */
 size_t bdda_plan_table_bytes(const bdda_plan* plan);
 int bdda_plan_attach_tables(bdda_plan* plan, void* dev_tables, void* stream);
+/* Bounded waits of this plan's pass kernels that ran out (a CTA whose tile
+ * copy did not land in time counts one and leaves its pencil unwritten): 0
+ * in every correct run.  The counter lives in the table buffer, zeroed by
+ * bdda_plan_attach_tables.  Synchronises the stream. */
+int bdda_plan_wait_timeouts(const bdda_plan* plan, unsigned int* count, void* stream);
 
 /* Launch shape of the pencil passes (no counterpart in the reference; used by
  * the autotuner).  kind: 0 forward passes (Z, Y), 1 X pass (forward, Green
@@ -90,13 +95,17 @@ int bdda_plan_attach_tables(bdda_plan* plan, void* dev_tables, void* stream);
 int bdda_tune_set(int prec, int kind, size_t smem_budget, int threads);
 int bdda_tune_get(int prec, int kind, size_t* smem_budget, int* threads);
 /* Per-pass launch choice for passes of (prec, kind) over an axis of length M
- * at block width L: column tile width lt (2, 4, 8; 0 = the smem_budget rule)
+ * at block width L: column tile width lt (2, 4, 8, 16; 0 = the smem_budget rule)
  * and kernel variant (0 = the first specialised kernel compiled for the radix
  * sequence; k in 1..8 = the one of 256 threads compiled for k resident CTAs
  * per SM; k + 16 * (threads / 32) = the one of that CTA size; 512 + either
  * = a complex64 kernel whose jobs take two adjacent columns, used when L is
- * even and the pass's field pointers are 16-byte aligned; -1 = the generic
- * run-time-radix kernel).  Process-wide; set by bdda_autotune. */
+ * even and the pass's field pointers are 16-byte aligned; 1024 + any of
+ * these = the same kernel with the tile's first read done by a bulk tensor
+ * copy (TMA), used when the pass's source is dense and 16-byte aligned, the
+ * plain kernel otherwise; -1 = the generic run-time-radix kernel).
+ * lt 16 exists as specialised kernels only.  Process-wide; set by
+ * bdda_autotune. */
 int bdda_tune_pass(int prec, int kind, int M, int L, int lt, int variant);
 int bdda_tune_pass_get(int prec, int kind, int M, int L, int* lt, int* variant);
 /* Variant ids (as bdda_tune_pass) of the specialised kernels compiled for the

@@ -153,8 +153,9 @@ def test_mixed_settings_round_trip_and_reject_bad_values():
 
 def test_pass_variant_lists_name_the_compiled_kernels():
     """Host-only: for the x=20 particle's grid (192 x 224 x 350) every complex64
-    pass has one-column and column-pair (id >= 512) specialised kernels at
-    tile width 8, complex128 only one-column ones; the count is reported even
+    pass has one-column and column-pair (id bit 512) specialised kernels at
+    tile width 8, complex128 only one-column ones; the passes with a dense
+    source also have TMA-filled ones (id >= 1024); the count is reported even
     when cap is 0; bad arguments are rejected."""
     lib = _lib.load()
     h = C.c_void_p()
@@ -169,11 +170,19 @@ def test_pass_variant_lists_name_the_compiled_kernels():
             assert any(v >= 512 for v in ids) and any(0 < v < 512 for v in ids), (kind, axis, ids)
             assert len(set(ids)) == len(ids)
             assert lib.bdda_tune_pass_variants(h, 1, kind, axis, 8, None, 0, C.byref(n)) == 0 and n.value == len(ids)
+            # dense-source passes (all but the gathering Z pass) also have TMA-filled kernels (id >= 1024)
+            assert any(v >= 1024 for v in ids) == ((kind, axis) != (0, 2)), (kind, axis, ids)
             assert lib.bdda_tune_pass_variants(h, 0, kind, axis, 4, buf, 64, C.byref(n)) == 0
             ids = list(buf[:n.value])
-            assert ids and all(v < 512 for v in ids) and len(set(ids)) == len(ids), (kind, axis, ids)
+            assert ids and all(not (v & 512) for v in ids) and len(set(ids)) == len(ids), (kind, axis, ids)
+            assert any(v >= 1024 for v in ids) == ((kind, axis) != (0, 2)), (kind, axis, ids)
         assert lib.bdda_tune_pass_variants(h, 1, 3, 0, 8, buf, 64, C.byref(n)) == _lib.BAD_ARG
         assert lib.bdda_tune_pass_variants(h, 1, 1, 3, 8, buf, 64, C.byref(n)) == _lib.BAD_ARG
         assert lib.bdda_tune_pass_variants(None, 1, 1, 0, 8, buf, 64, C.byref(n)) == _lib.BAD_ARG
+        # the wait-timeout counter lives in the device tables: none attached yet
+        cnt = C.c_uint()
+        assert lib.bdda_plan_wait_timeouts(h, C.byref(cnt), None) == _lib.NO_WORKSPACE
+        assert lib.bdda_plan_wait_timeouts(h, None, None) == _lib.BAD_ARG
+        assert lib.bdda_plan_wait_timeouts(None, C.byref(cnt), None) == _lib.BAD_ARG
     finally:
         lib.bdda_plan_destroy(h)

@@ -119,3 +119,39 @@ def test_every_compiled_complex64_variant_gives_the_product(case):
         for kind, axis in ((0, 2), (0, 1), (1, 0), (2, 1), (2, 2)):
             lib.bdda_tune_pass(1, kind, plan.m[axis], 64, 0, 0)
     assert tested >= 20
+    assert plan.wait_timeouts() == 0
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_tma_filled_tiles_give_the_plain_kernels_product(case, prec):
+    """Each kernel whose tile is filled by a bulk tensor copy (id >= 1024)
+    gives the product of the same kernel with the first stage's global loads
+    (id - 1024) to rounding (the copy moves the same values, zero-filled past
+    the source rows and columns as the loads are; the arithmetic is the same
+    code); no bounded wait of the copies ran out."""
+    import ctypes as C
+    lib = case["lib"].load()
+    plan = case["plan"]
+    lt = 8 if prec == 1 else 4
+    tested = 0
+    try:
+        for kind, axis in ((0, 1), (1, 0), (2, 1), (2, 2)):
+            M = plan.m[axis]
+            buf, n = (C.c_int * 64)(), C.c_int()
+            assert lib.bdda_tune_pass_variants(plan.handle, prec, kind, axis, lt, buf, 64, C.byref(n)) == 0
+            tma = [v for v in buf[:n.value] if v >= 1024]
+            assert tma, (kind, axis, list(buf[:n.value]))
+            for v in tma:
+                assert lib.bdda_tune_pass(prec, kind, M, 64, lt, v - 1024) == 0
+                Yp = _mvp(case, prec, case["S"])
+                assert lib.bdda_tune_pass(prec, kind, M, 64, lt, v) == 0
+                Yt = _mvp(case, prec, case["S"])
+                err = (Yt - Yp).abs().max().item() / Yp.abs().max().item()
+                assert err <= (1e-15 if prec == 0 else 1e-7), (prec, kind, axis, v, err)
+                tested += 1
+            assert lib.bdda_tune_pass(prec, kind, M, 64, 0, 0) == 0
+    finally:
+        for kind, axis in ((0, 2), (0, 1), (1, 0), (2, 1), (2, 2)):
+            lib.bdda_tune_pass(prec, kind, plan.m[axis], 64, 0, 0)
+    assert tested >= 4
+    assert plan.wait_timeouts() == 0
