@@ -496,6 +496,8 @@ int fixed_launch(const PassArgs& a0, int64_t P0, cudaStream_t st) {
   { PREC, KIND, LT, MINB, 512 + MINB + 16 * ((NT) / 32), {R0, R1, R2, R3},                        \
     &fixed_launch<float2, KIND, LT, MINB, NT, 1, R0, R1, R2, R3>, 1 }
 // The same with the tile's first read by a bulk tensor copy: ids + 1024.
+#define BDDA_FIXED_TMA(T, PREC, KIND, LT, MINB, R0, R1, R2, R3) \
+  { PREC, KIND, LT, MINB, 1024 + MINB, {R0, R1, R2, R3}, &fixed_launch<T, KIND, LT, MINB, 256, 0, R0, R1, R2, R3, 1>, 0 }
 #define BDDA_FIXED_TMA_NT(T, PREC, KIND, LT, MINB, NT, R0, R1, R2, R3)                          \
   { PREC, KIND, LT, MINB, 1024 + MINB + 16 * ((NT) / 32), {R0, R1, R2, R3},                       \
     &fixed_launch<T, KIND, LT, MINB, NT, 0, R0, R1, R2, R3, 1>, 0 }

@@ -17,11 +17,16 @@ static const FixedKernel kTableI[] = {
     BDDA_FIXED_TMA_PAIR(1, K_INV, 8, 4, 224, 10, 7, 5, 1),
     BDDA_FIXED_TMA_PAIR(1, K_CONV, 8, 4, 160, 8, 8, 3, 1),
     BDDA_FIXED_TMA_PAIR(1, K_CONV, 8, 3, 192, 8, 8, 3, 1),
-    // complex128, tile width 4
+    // complex128, tile width 4 (and 8 for the X pass)
     BDDA_FIXED_TMA_NT(double2, 0, K_FWD, 4, 2, 384, 8, 7, 4, 1),
     BDDA_FIXED_TMA_NT(double2, 0, K_INV, 4, 2, 384, 8, 7, 4, 1),
+    BDDA_FIXED_TMA(double2, 0, K_FWD, 4, 4, 8, 7, 4, 1),
+    BDDA_FIXED_TMA(double2, 0, K_INV, 4, 4, 8, 7, 4, 1),
+    BDDA_FIXED_TMA(double2, 0, K_FWD, 4, 3, 8, 7, 4, 1),
+    BDDA_FIXED_TMA(double2, 0, K_INV, 4, 3, 8, 7, 4, 1),
     BDDA_FIXED_TMA_NT(double2, 0, K_INV, 4, 3, 224, 10, 7, 5, 1),
     BDDA_FIXED_TMA_NT(double2, 0, K_CONV, 4, 2, 288, 8, 8, 3, 1),
+    BDDA_FIXED_TMA_NT(double2, 0, K_CONV, 8, 2, 288, 8, 8, 3, 1),
 };
 
 const FixedKernel* fixed_table_i(int* n) {

@@ -1264,6 +1264,17 @@ size_t bdda_solver_workspace_bytes(const bdda_plan* p, int solver, int prec, int
   return layout(p, prec, L, n_occ).total;
 }
 
+// A solve whose pass kernels gave up waiting for a tile copy left pencils
+// unwritten: its result is not trusted (BDDA_TIMEOUT), whatever it converged to.
+static int wait_status(const bdda_plan* p, int status, cudaStream_t st) {
+  if (status == BDDA_BAD_ARG || status == BDDA_NO_WORKSPACE || status == BDDA_CUDA_ERROR) return status;
+  unsigned int n = 0;
+  if (cudaMemcpyAsync(&n, plan_err(p), sizeof(n), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess)
+    return BDDA_CUDA_ERROR;
+  return n ? BDDA_TIMEOUT : status;
+}
+
 int bdda_solve(const bdda_plan* p, int solver, int prec, int L, int n_occ, const void* ghat,
                const int32_t* cell_map, const void* diag, const void* B, const void* X0, double tol,
                int itermax, void* X, int* iter_fin, double* err_fin, double* history, void* work,
@@ -1281,15 +1292,19 @@ int bdda_solve(const bdda_plan* p, int solver, int prec, int L, int n_occ, const
   }
   const cudaStream_t st = (cudaStream_t)stream;
   if (prec == BDDA_C128)
-    return run_solver<double2>(solver, p, L, n_occ, ghat, cell_map, static_cast<const double2*>(diag),
-                               static_cast<const double2*>(B), static_cast<const double2*>(X0), tol,
-                               itermax, static_cast<double2*>(X), iter_fin, err_fin, history, work,
-                               work_bytes, st);
+    return wait_status(p,
+                       run_solver<double2>(solver, p, L, n_occ, ghat, cell_map, static_cast<const double2*>(diag),
+                                           static_cast<const double2*>(B), static_cast<const double2*>(X0), tol,
+                                           itermax, static_cast<double2*>(X), iter_fin, err_fin, history, work,
+                                           work_bytes, st),
+                       st);
   if (prec == BDDA_C64)
-    return run_solver<float2>(solver, p, L, n_occ, ghat, cell_map, static_cast<const double2*>(diag),
-                              static_cast<const double2*>(B), static_cast<const double2*>(X0), tol,
-                              itermax, static_cast<double2*>(X), iter_fin, err_fin, history, work,
-                              work_bytes, st);
+    return wait_status(p,
+                       run_solver<float2>(solver, p, L, n_occ, ghat, cell_map, static_cast<const double2*>(diag),
+                                          static_cast<const double2*>(B), static_cast<const double2*>(X0), tol,
+                                          itermax, static_cast<double2*>(X), iter_fin, err_fin, history, work,
+                                          work_bytes, st),
+                       st);
   return BDDA_BAD_ARG;
 }
 
@@ -1334,10 +1349,13 @@ int bdda_refine_solve(const bdda_plan* p, int solver, int L, int n_occ, const vo
   // recursion with FP64 reliable updates (replacement factor inner_tol)
   const bool restart = solver == BDDA_COCG_RQ || max_outer > 0;
   if (max_outer < 0) max_outer = -max_outer;
-  return run_refine(solver, restart, p, L, n_occ, ghat_c128, ghat_c64, cell_map, static_cast<const double2*>(diag),
-                    static_cast<const double2*>(B), static_cast<const double2*>(X0), tol, itermax, inner_tol,
-                    max_outer, static_cast<double2*>(X), iter_fin, err_fin, history, work, work_bytes,
-                    (cudaStream_t)stream);
+  return wait_status(p,
+                     run_refine(solver, restart, p, L, n_occ, ghat_c128, ghat_c64, cell_map,
+                                static_cast<const double2*>(diag), static_cast<const double2*>(B),
+                                static_cast<const double2*>(X0), tol, itermax, inner_tol, max_outer,
+                                static_cast<double2*>(X), iter_fin, err_fin, history, work, work_bytes,
+                                (cudaStream_t)stream),
+                     (cudaStream_t)stream);
 }
 
 int bdda_tune_solver_graphs(int on) {
@@ -1377,10 +1395,12 @@ int bdda_mixed_solve(const bdda_plan* p, int solver, int L, int n_occ, const voi
       (solver != BDDA_BICGSTAB && solver != BDDA_COCG_RQ))
     return BDDA_BAD_ARG;
   if (!p->dev_tables || !work) return BDDA_NO_WORKSPACE;
-  return run_mixed(solver, p, L, n_occ, ghat_c128, ghat_c64, cell_map, static_cast<const double2*>(diag),
-                   static_cast<const double2*>(B), static_cast<const double2*>(X0), tol, itermax, max_outer,
-                   static_cast<double2*>(X), iter_fin, err_fin, history, work, work_bytes,
-                   static_cast<cudaStream_t>(stream));
+  return wait_status(p,
+                     run_mixed(solver, p, L, n_occ, ghat_c128, ghat_c64, cell_map, static_cast<const double2*>(diag),
+                               static_cast<const double2*>(B), static_cast<const double2*>(X0), tol, itermax,
+                               max_outer, static_cast<double2*>(X), iter_fin, err_fin, history, work, work_bytes,
+                               static_cast<cudaStream_t>(stream)),
+                     static_cast<cudaStream_t>(stream));
 }
 
 size_t bdda_dda_workspace_bytes(const bdda_plan* p, int mode, int L, int n_occ) {
@@ -1441,14 +1461,17 @@ int bdda_dda_solve(const bdda_plan* p, const bdda_dda_problem* prob, int solver,
     BDDA_CUDA_TRY(cudaMemsetAsync(obs, 0, (size_t)L * 12 * sizeof(double), st));
     return BDDA_NOT_CONVERGED;
   }
+  int status;
   if (mode == BDDA_BATCH_MIXED)
-    return run_mixed(solver, p, L, n_occ, ghat_c128, ghat_c64, cell_map, nullptr, nullptr, X0d, tol, itermax,
-                     max_outer, Xd, iter_fin, err_fin, history, work, base, st, &ph);
-  if (mode == BDDA_BATCH_C128)
-    return run_solver<double2>(solver, p, L, n_occ, ghat_c128, cell_map, nullptr, nullptr, X0d, tol, itermax, Xd,
-                               iter_fin, err_fin, history, work, base, st, &ph);
-  return run_solver<float2>(solver, p, L, n_occ, ghat_c64, cell_map, nullptr, nullptr, X0d, tol, itermax, Xd,
-                            iter_fin, err_fin, history, work, base, st, &ph);
+    status = run_mixed(solver, p, L, n_occ, ghat_c128, ghat_c64, cell_map, nullptr, nullptr, X0d, tol, itermax,
+                       max_outer, Xd, iter_fin, err_fin, history, work, base, st, &ph);
+  else if (mode == BDDA_BATCH_C128)
+    status = run_solver<double2>(solver, p, L, n_occ, ghat_c128, cell_map, nullptr, nullptr, X0d, tol, itermax, Xd,
+                                 iter_fin, err_fin, history, work, base, st, &ph);
+  else
+    status = run_solver<float2>(solver, p, L, n_occ, ghat_c64, cell_map, nullptr, nullptr, X0d, tol, itermax, Xd,
+                                iter_fin, err_fin, history, work, base, st, &ph);
+  return wait_status(p, status, st);
 }
 
 }  // extern "C"

@@ -84,7 +84,8 @@ int bdda_plan_attach_tables(bdda_plan* plan, void* dev_tables, void* stream);
 /* Bounded waits of this plan's pass kernels that ran out (a CTA whose tile
  * copy did not land in time counts one and leaves its pencil unwritten): 0
  * in every correct run.  The counter lives in the table buffer, zeroed by
- * bdda_plan_attach_tables.  Synchronises the stream. */
+ * bdda_plan_attach_tables; the solve entry points read it when they finish
+ * and return BDDA_TIMEOUT if it is not 0.  Synchronises the stream. */
 int bdda_plan_wait_timeouts(const bdda_plan* plan, unsigned int* count, void* stream);
 
 /* Launch shape of the pencil passes (no counterpart in the reference; used by

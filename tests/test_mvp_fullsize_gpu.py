@@ -132,23 +132,24 @@ def test_tma_filled_tiles_give_the_plain_kernels_product(case, prec):
     import ctypes as C
     lib = case["lib"].load()
     plan = case["plan"]
-    lt = 8 if prec == 1 else 4
     tested = 0
     try:
         for kind, axis in ((0, 1), (1, 0), (2, 1), (2, 2)):
             M = plan.m[axis]
-            buf, n = (C.c_int * 64)(), C.c_int()
-            assert lib.bdda_tune_pass_variants(plan.handle, prec, kind, axis, lt, buf, 64, C.byref(n)) == 0
-            tma = [v for v in buf[:n.value] if v >= 1024]
-            assert tma, (kind, axis, list(buf[:n.value]))
-            for v in tma:
-                assert lib.bdda_tune_pass(prec, kind, M, 64, lt, v - 1024) == 0
-                Yp = _mvp(case, prec, case["S"])
-                assert lib.bdda_tune_pass(prec, kind, M, 64, lt, v) == 0
-                Yt = _mvp(case, prec, case["S"])
-                err = (Yt - Yp).abs().max().item() / Yp.abs().max().item()
-                assert err <= (1e-15 if prec == 0 else 1e-7), (prec, kind, axis, v, err)
-                tested += 1
+            n_tma = 0
+            for lt in (4, 8):
+                buf, n = (C.c_int * 64)(), C.c_int()
+                assert lib.bdda_tune_pass_variants(plan.handle, prec, kind, axis, lt, buf, 64, C.byref(n)) == 0
+                for v in [v for v in buf[:n.value] if v >= 1024]:
+                    assert lib.bdda_tune_pass(prec, kind, M, 64, lt, v - 1024) == 0
+                    Yp = _mvp(case, prec, case["S"])
+                    assert lib.bdda_tune_pass(prec, kind, M, 64, lt, v) == 0
+                    Yt = _mvp(case, prec, case["S"])
+                    err = (Yt - Yp).abs().max().item() / Yp.abs().max().item()
+                    assert err <= (1e-15 if prec == 0 else 1e-7), (prec, kind, axis, lt, v, err)
+                    n_tma += 1
+            assert n_tma, (prec, kind, axis)
+            tested += n_tma
             assert lib.bdda_tune_pass(prec, kind, M, 64, 0, 0) == 0
     finally:
         for kind, axis in ((0, 2), (0, 1), (1, 0), (2, 1), (2, 2)):

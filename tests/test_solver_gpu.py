@@ -346,9 +346,10 @@ def test_graph_driven_loop_matches_the_host_loop(mods, solver, prec):
     assert res[1][2] == res[0][2]
     assert res[1][3] == res[0][3]
     assert np.array_equal(res[1][0], res[0][0])
-    # the launch counter counts the kernels the graph ran, as the host loop does
-    # (COCG's graph adds no kernel: it copies the new Q in place of the swap)
-    assert abs(res[1][4] - res[0][4]) <= 4
+    # the launch counter counts the kernels the graph ran: the host loop's,
+    # plus the loop-condition kernel once per iteration (the host loop reads
+    # the residual instead; COCG's in-place copy of the new Q is no kernel)
+    assert abs((res[1][4] - res[0][4]) - (res[1][1] + 1)) <= 2, (res[1][4], res[0][4], res[1][1])
 
 
 def test_graph_driven_loop_stops_at_itermax(mods):
