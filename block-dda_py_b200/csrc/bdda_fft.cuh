@@ -124,6 +124,15 @@ template <> __device__ __forceinline__ constexpr double root_sin<16>(int j) {
   return t[j];
 }
 
+template <> __device__ __forceinline__ constexpr double root_cos<24>(int j) {
+  constexpr double t[24] = {1.000000000000000000000000, 0.9659258262890682867497432, 0.8660254037844386467637232, 0.7071067811865475244008444, 0.5000000000000000000000000, 0.2588190451025207623488988, 0.0, -0.2588190451025207623488988, -0.5000000000000000000000000, -0.7071067811865475244008444, -0.8660254037844386467637232, -0.9659258262890682867497432, -1.000000000000000000000000, -0.9659258262890682867497432, -0.8660254037844386467637232, -0.7071067811865475244008444, -0.5000000000000000000000000, -0.2588190451025207623488988, 0.0, 0.2588190451025207623488988, 0.5000000000000000000000000, 0.7071067811865475244008444, 0.8660254037844386467637232, 0.9659258262890682867497432};
+  return t[j];
+}
+template <> __device__ __forceinline__ constexpr double root_sin<24>(int j) {
+  constexpr double t[24] = {0.0, 0.2588190451025207623488988, 0.5000000000000000000000000, 0.7071067811865475244008444, 0.8660254037844386467637232, 0.9659258262890682867497432, 1.000000000000000000000000, 0.9659258262890682867497432, 0.8660254037844386467637232, 0.7071067811865475244008444, 0.5000000000000000000000000, 0.2588190451025207623488988, 0.0, -0.2588190451025207623488988, -0.5000000000000000000000000, -0.7071067811865475244008444, -0.8660254037844386467637232, -0.9659258262890682867497432, -1.000000000000000000000000, -0.9659258262890682867497432, -0.8660254037844386467637232, -0.7071067811865475244008444, -0.5000000000000000000000000, -0.2588190451025207623488988};
+  return t[j];
+}
+
 // ---- small DFTs on registers: y_q = sum_p v_p exp(-+2 pi i p q / R) ----------
 template <bool INV, typename T> __device__ __forceinline__ void dft2(T* v) {
   T a = v[0], b = v[1];
@@ -235,6 +244,7 @@ template <int R, bool INV, typename T> __device__ __forceinline__ void dft(T* v)
   else if constexpr (R == 12) dft_ab<4, 3, INV>(v);
   else if constexpr (R == 14) dft_ab<2, 7, INV>(v);
   else if constexpr (R == 16) dft_ab<4, 4, INV>(v);
+  else if constexpr (R == 24) dft_ab<8, 3, INV>(v);
   else static_assert(R == 2, "unsupported radix");
 }
 

@@ -234,6 +234,7 @@ __device__ __forceinline__ void fixed_mid(const PassArgs& a, const Pen& c, T* sm
 // a.err, waits (bounded again) for its copy to land and returns.
 struct TmaTile {
   int nbox, box_rows;
+  int rows;        // tile rows the boxes cover: [0, rows)
   int dim_of[3];   // dimension 2 + d of the map holds (row, p1, p0)[dim_of[d]]
 };
 
@@ -269,7 +270,7 @@ __device__ __forceinline__ void tma_issue(const PassArgs& a, const CUtensorMap* 
   const uint32_t bytes = (uint32_t)(tt.nbox * tt.box_rows * 3 * LT * (int)sizeof(T));
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes) : "memory");
   for (int b = 0; b < tt.nbox; ++b) {
-    const int row0 = b == 0 ? 0 : M - tt.box_rows;
+    const int row0 = b == 0 ? 0 : tt.rows - tt.box_rows;
     const int v[3] = {row0, (int)p1, (int)p0};
     int c[3];
 #pragma unroll
@@ -394,7 +395,7 @@ inline PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
   return fn;
 }
 
-// Rows of the one or two boxes that fill an M-row tile (box 1 starts at
+// Rows of the one or two boxes that fill M rows of a tile (box 1 starts at
 // M - box_rows, 128-byte aligned in the tile); false if M needs more.
 inline bool tile_boxes(int M, int row_bytes, int* nbox, int* box_rows) {
   if (M < 1) return false;
@@ -413,11 +414,14 @@ inline bool tile_boxes(int M, int row_bytes, int* nbox, int* box_rows) {
   return true;
 }
 
-// Tensor map of the tile copies of a pass.  False when the pass cannot use
-// them: a gathered or evaluated source, a source pointer, column offset or
-// stride that is not a 16-byte multiple, or a tile of more than two boxes.
+// Tensor map of the tile copies of a pass, covering tile rows [0, rows)
+// (rows = M: the source rows and the zero rows after them; rows = n_in: the
+// source rows only, for kernels that never read the others).  False when the
+// pass cannot use them: a gathered or evaluated source, a source pointer,
+// column offset or stride that is not a 16-byte multiple, or more than two
+// boxes.
 template <typename T, int KIND, int LT>
-bool make_tile_map(const PassArgs& a, int64_t P0, int M, CUtensorMap* tm, TmaTile* tt) {
+bool make_tile_map(const PassArgs& a, int64_t P0, int rows, CUtensorMap* tm, TmaTile* tt) {
   constexpr int E = sizeof(T) / 8;
   const int64_t s = sizeof(T);
   if ((KIND == K_FWD && a.cell_map) || a.green || !a.src) return false;
@@ -428,7 +432,7 @@ bool make_tile_map(const PassArgs& a, int64_t P0, int M, CUtensorMap* tm, TmaTil
   for (int64_t st : strides)
     if (st <= 0 || st % 16 || st >= ((int64_t)1 << 40)) return false;
   int nbox, box_rows;
-  if (!tile_boxes(M, 3 * LT * (int)s, &nbox, &box_rows)) return false;
+  if (rows < 1 || !tile_boxes(rows, 3 * LT * (int)s, &nbox, &box_rows)) return false;
   auto enc = tensor_map_encoder();
   if (!enc) return false;
   // dimensions 2..4: (row, p1, p0) ordered by stride
@@ -450,6 +454,7 @@ bool make_tile_map(const PassArgs& a, int64_t P0, int M, CUtensorMap* tm, TmaTil
   }
   tt->nbox = nbox;
   tt->box_rows = box_rows;
+  tt->rows = rows;
   const CUresult r = enc(tm, CU_TENSOR_MAP_DATA_TYPE_UINT64, 5, const_cast<void*>(a.src), gdim, gstride, box, estr,
                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);

@@ -99,7 +99,7 @@ static int launch_lt(PassArgs a, int64_t P0, cudaStream_t st) {
 
 static int g_use_fixed = 1;   // specialised kernels on (bdda_tune_fixed)
 
-static constexpr int kFixedTables = 9;
+static constexpr int kFixedTables = 10;
 
 static const FixedKernel* fixed_table(int t, int* n) {
   switch (t) {
@@ -111,7 +111,8 @@ static const FixedKernel* fixed_table(int t, int* n) {
     case 5: return fixed_table_f(n);
     case 6: return fixed_table_g(n);
     case 7: return fixed_table_h(n);
-    default: return fixed_table_i(n);
+    case 8: return fixed_table_i(n);
+    default: return fixed_table_j(n);
   }
 }
 
@@ -549,7 +550,7 @@ int bdda_tune_set(int prec, int kind, size_t smem_budget, int threads) {
 
 int bdda_tune_pass(int prec, int kind, int M, int L, int lt, int variant) {
   if (prec < 0 || prec > 1 || kind < 0 || kind > 2 || M < 1 || L < 1 || L > kMaxL ||
-      (lt != 0 && lt != 2 && lt != 4 && lt != 8 && lt != 16) || variant < -1 || variant >= 2048)
+      (lt != 0 && lt != 2 && lt != 4 && lt != 8 && lt != 16) || variant < -1 || variant >= 4096)
     return BDDA_BAD_ARG;
   set_pass_tune({prec, kind, M, L, lt, variant});
   return BDDA_OK;

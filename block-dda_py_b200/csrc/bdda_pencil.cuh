@@ -454,6 +454,7 @@ const FixedKernel* fixed_table_f(int* n);
 const FixedKernel* fixed_table_g(int* n);
 const FixedKernel* fixed_table_h(int* n);
 const FixedKernel* fixed_table_i(int* n);
+const FixedKernel* fixed_table_j(int* n);
 
 
 }  // namespace bdda

@@ -1,0 +1,162 @@
+// X pass (forward x transform, 3x3 Green multiply, inverse x transform) of an
+// axis of length M = A * B in two register stages instead of the plan's
+// radix sequence.
+//
+// The specialised X-pass kernels run the plan's stages ([8,8,3] for the
+// x=20 particle's 192-point axis): four shared-memory round trips of the
+// tile, which ncu shows as the pass's limit together with the FP32 issue
+// rate (shared wavefronts ~66 % busy).  Here the transform of a column is
+//   X[k + A k2] = sum_j W_B^(j k2) w^(j k) sum_q x[j + B q] W_A^(q k)
+// (j < B, q, k < A, k2 < B, w = exp(-2 pi i / M)):
+//   stage 1: per (j, column) a register DFT_A over rows j + B q, the twiddles
+//            w^(j k), written to rows j + B k;
+//   middle:  per (k, column) a register DFT_B over rows B k + j of the three
+//            components, the Green multiply at frequency k + A k2, the
+//            inverse DFT_B, written back;
+//   stage 1 inverse: per (j, column) the conjugate twiddles and the inverse
+//            DFT_A, stored to the rows below n_out.
+// That is two round trips instead of four.  The Green's spectrum keeps the
+// plan's storage order (position of frequency f under the plan's digit
+// reversal, radices P0 P1 P2), so the kernel drops into a plan whose x axis
+// is factored [P0, P1, P2] and gives the same product to rounding.  Stage 1
+// skips the source rows at or past n_in (zero), so a TMA copy needs only
+// those rows.
+#pragma once
+#include "bdda_fixed.cuh"
+
+namespace bdda {
+
+// Position in the plan's digit-reversed storage of frequency f (three DIF
+// stages of radices P0, P1, P2).
+template <int P0, int P1, int P2>
+__device__ __forceinline__ int plan_position(int f) {
+  constexpr int M = P0 * P1 * P2;
+  const int d0 = f % P0, d1 = (f / P0) % P1, d2 = f / (P0 * P1);
+  return d0 * (M / P0) + d1 * (M / (P0 * P1)) + d2;
+}
+
+template <typename T, int LT, int NT, int MINB, int A, int B, int P0, int P1, int P2, int TMA>
+__global__ void __launch_bounds__(NT, MINB) xconv2_kernel(const PassArgs a, const __grid_constant__ CUtensorMap tm,
+                                                          const TmaTile tt) {
+  constexpr int M = A * B, W = 3 * LT;
+  static_assert(M == P0 * P1 * P2, "two-stage split and plan radices describe one axis");
+  extern __shared__ __align__(128) unsigned char smraw[];
+  const bool from_tile = TMA && (smem_u32(pencil_tile<T, LT>(smraw, M)) & 127) == 0;
+  if constexpr (TMA) {
+    if (from_tile && threadIdx.x == 0) tma_issue<T, K_CONV, LT>(a, &tm, tt, smraw, M, blockIdx.x);
+  }
+  T *tw, *sm, *gs;
+  int32_t* cm;
+  stage_constants<T, K_CONV, LT>(a, smraw, M, &tw, &sm, &gs, &cm, blockIdx.x);
+  const Pen c = pen_of_block<T>(a, cm, blockIdx.x);
+  if constexpr (TMA) {
+    if (from_tile) {
+      const uint32_t bar = smem_u32(pencil_barrier<T, K_CONV, LT>(smraw, M));
+      const bool landed = mbar_wait_bounded(bar, 0, kTmaWaitLimit);
+      if (__syncthreads_or(!landed)) {   // the whole CTA leaves together
+        if (threadIdx.x == 0) {
+          if (a.err) atomicAdd(a.err, 1u);
+          mbar_wait_bounded(bar, 0, kTmaWaitLimit);
+        }
+        return;
+      }
+    }
+  }
+  cp_async_wait<0>();   // the Green's pencil
+  __syncthreads();
+  const int n_in = a.n_in;
+  // stage 1, forward
+#pragma unroll 1
+  for (int job = threadIdx.x; job < B * W; job += NT) {
+    const int col = job % W, j = job / W;
+    T v[A];
+#pragma unroll
+    for (int q = 0; q < A; ++q) {
+      const int row = j + B * q;
+      if (row < n_in) v[q] = from_tile ? sm[row * W + col] : gload<K_CONV, T, LT>(a, c, row, col);
+      else v[q] = mkc<T>(0, 0);
+    }
+    dft<A, false>(v);
+#pragma unroll
+    for (int k = 1; k < A; ++k) v[k] = cmul(v[k], tw[j * k]);
+#pragma unroll
+    for (int k = 0; k < A; ++k) sm[(j + B * k) * W + col] = v[k];
+  }
+  __syncthreads();
+  // middle: DFT_B of the three components, Green multiply, inverse DFT_B
+#pragma unroll 1
+  for (int job = threadIdx.x; job < A * LT; job += NT) {
+    const int li = job % LT, k = job / LT;
+    T y[3][B];
+#pragma unroll
+    for (int comp = 0; comp < 3; ++comp) {
+#pragma unroll
+      for (int jj = 0; jj < B; ++jj) y[comp][jj] = sm[(B * k + jj) * W + comp * LT + li];
+      dft<B, false>(y[comp]);
+    }
+#pragma unroll
+    for (int k2 = 0; k2 < B; ++k2) {
+      const T* g = gs + plan_position<P0, P1, P2>(k + A * k2) * 6;
+      const T gxx = g[0], gxy = g[1], gxz = g[2], gyy = g[3], gyz = g[4], gzz = g[5];
+      const T v0 = y[0][k2], v1 = y[1][k2], v2 = y[2][k2];
+      y[0][k2] = cadd(cadd(cmul(gxx, v0), cmul(gxy, v1)), cmul(gxz, v2));
+      y[1][k2] = cadd(cadd(cmul(gxy, v0), cmul(gyy, v1)), cmul(gyz, v2));
+      y[2][k2] = cadd(cadd(cmul(gxz, v0), cmul(gyz, v1)), cmul(gzz, v2));
+    }
+#pragma unroll
+    for (int comp = 0; comp < 3; ++comp) {
+      dft<B, true>(y[comp]);
+#pragma unroll
+      for (int jj = 0; jj < B; ++jj) sm[(B * k + jj) * W + comp * LT + li] = y[comp][jj];
+    }
+  }
+  __syncthreads();
+  // stage 1, inverse: rows below n_out to global memory
+#pragma unroll 1
+  for (int job = threadIdx.x; job < B * W; job += NT) {
+    const int col = job % W, j = job / W;
+    T v[A];
+    v[0] = sm[j * W + col];
+#pragma unroll
+    for (int k = 1; k < A; ++k) v[k] = cmulc(sm[(j + B * k) * W + col], tw[j * k]);
+    dft<A, true>(v);
+#pragma unroll
+    for (int q = 0; q < A; ++q) gstore<K_CONV, T, LT>(a, c, j + B * q, col, v[q]);
+  }
+}
+
+template <typename T, int LT, int NT, int MINB, int A, int B, int P0, int P1, int P2, int TMA>
+int xconv2_launch(const PassArgs& a0, int64_t P0n, cudaStream_t st) {
+  static_assert(NT % 32 == 0 && NT <= 512 && MINB >= 1 && MINB < 16, "variant id encodes whole warps and MINB < 16");
+  constexpr int M = A * B;
+  PassArgs a = a0;
+  if (a.ax.M != M || a.ax.nst != 3 || a.ax.rad[0] != P0 || a.ax.rad[1] != P1 || a.ax.rad[2] != P2 || a.green ||
+      a.n_in > M)
+    return BDDA_BAD_ARG;
+  a.ntile = (a.L + LT - 1) / LT;
+  CUtensorMap tm;
+  memset(&tm, 0, sizeof(tm));
+  TmaTile tt;
+  memset(&tt, 0, sizeof(tt));
+  if (TMA && !make_tile_map<T, K_CONV, LT>(a, P0n, a.n_in, &tm, &tt))   // the plain loads
+    return xconv2_launch<T, LT, NT, MINB, A, B, P0, P1, P2, 0>(a0, P0n, st);
+  auto kern = xconv2_kernel<T, LT, NT, MINB, A, B, P0, P1, P2, TMA>;
+  const size_t smem = (size_t)pencil_smem_bytes<T>(M, LT, K_CONV);
+  if (smem > 227 * 1024) return BDDA_BAD_ARG;
+  const int64_t nblk = P0n * a.P1 * a.ntile;
+  if (nblk <= 0) return BDDA_OK;
+  if (nblk > 0x7fffffff) return BDDA_BAD_ARG;
+  BDDA_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  kern<<<(unsigned)nblk, NT, smem, st>>>(a, tm, tt);
+  BDDA_CUDA_TRY(cudaGetLastError());
+  count_launch();
+  return BDDA_OK;
+}
+
+// Table entry (kind K_CONV, the plan's radix sequence): variant id 2048 +
+// MINB + 16 NT/32, + 1024 with the TMA-filled tile.
+#define BDDA_XCONV2(T, PREC, LT, MINB, NT, A, B, P0, P1, P2, TMA)                                 \
+  { PREC, K_CONV, LT, MINB, 2048 + 1024 * (TMA) + MINB + 16 * ((NT) / 32), {P0, P1, P2, 1},         \
+    &xconv2_launch<T, LT, NT, MINB, A, B, P0, P1, P2, TMA>, 0 }
+
+}  // namespace bdda

@@ -104,7 +104,10 @@ int bdda_tune_get(int prec, int kind, size_t* smem_budget, int* threads);
  * even and the pass's field pointers are 16-byte aligned; 1024 + any of
  * these = the same kernel with the tile's first read done by a bulk tensor
  * copy (TMA), used when the pass's source is dense and 16-byte aligned, the
- * plain kernel otherwise; -1 = the generic run-time-radix kernel).
+ * plain kernel otherwise; 2048 + (0 or 1024) + MINB + 16 * (threads / 32) =
+ * an X-pass kernel that transforms the axis in two register stages (a
+ * 192-point axis as 24 x 8) instead of the plan's radix sequence, with or
+ * without the TMA-filled tile; -1 = the generic run-time-radix kernel).
  * lt 16 exists as specialised kernels only.  Process-wide; set by
  * bdda_autotune. */
 int bdda_tune_pass(int prec, int kind, int M, int L, int lt, int variant);

@@ -140,7 +140,7 @@ def test_tma_filled_tiles_give_the_plain_kernels_product(case, prec):
             for lt in (4, 8):
                 buf, n = (C.c_int * 64)(), C.c_int()
                 assert lib.bdda_tune_pass_variants(plan.handle, prec, kind, axis, lt, buf, 64, C.byref(n)) == 0
-                for v in [v for v in buf[:n.value] if v >= 1024]:
+                for v in [v for v in buf[:n.value] if v & 1024]:
                     assert lib.bdda_tune_pass(prec, kind, M, 64, lt, v - 1024) == 0
                     Yp = _mvp(case, prec, case["S"])
                     assert lib.bdda_tune_pass(prec, kind, M, 64, lt, v) == 0
@@ -154,5 +154,38 @@ def test_tma_filled_tiles_give_the_plain_kernels_product(case, prec):
     finally:
         for kind, axis in ((0, 2), (0, 1), (1, 0), (2, 1), (2, 2)):
             lib.bdda_tune_pass(prec, kind, plan.m[axis], 64, 0, 0)
+    assert tested >= 4
+    assert plan.wait_timeouts() == 0
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_two_stage_x_pass_gives_the_plan_stage_product(case, prec):
+    """The X-pass kernels that transform the 192-point axis as 24 x 8 (ids
+    from 2048; the plan's stages are [8,8,3]) give the product of the
+    generic run-time-radix kernels: 1e-12 in complex128, 1e-6 in complex64
+    (different rounding order); with and without the TMA-filled tile."""
+    import ctypes as C
+    lib = case["lib"].load()
+    plan = case["plan"]
+    M = plan.m[0]
+    lib.bdda_tune_fixed(0)
+    try:
+        Yg = _mvp(case, prec, case["S"])
+    finally:
+        lib.bdda_tune_fixed(1)
+    scale = Yg.abs().max().item()
+    tested = 0
+    try:
+        for lt in (4, 8):
+            buf, n = (C.c_int * 64)(), C.c_int()
+            assert lib.bdda_tune_pass_variants(plan.handle, prec, 1, 0, lt, buf, 64, C.byref(n)) == 0
+            for v in [v for v in buf[:n.value] if v >= 2048]:
+                assert lib.bdda_tune_pass(prec, 1, M, 64, lt, v) == 0
+                Y = _mvp(case, prec, case["S"])
+                err = (Y - Yg).abs().max().item() / scale
+                assert err < (1e-12 if prec == 0 else 1e-6), (prec, lt, v, err)
+                tested += 1
+    finally:
+        lib.bdda_tune_pass(prec, 1, M, 64, 0, 0)
     assert tested >= 4
     assert plan.wait_timeouts() == 0
