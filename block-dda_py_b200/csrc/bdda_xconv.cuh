@@ -8,8 +8,8 @@
 //   X[k + A k2] = sum_j W_B^(j k2) w^(j k) sum_q x[j + B q] W_A^(q k)
 // (j < B, q, k < A, k2 < B, w = exp(-2 pi i / M)):
 //   stage 1: per (j, column) a register DFT_A over rows j + B q, the twiddles
-//            w^(j k), written to rows j A + k;
-//   middle:  per (k, column) a register DFT_B over rows j A + k of the three
+//            w^(j k), written to the rows of (j, k) (xrow);
+//   middle:  per (k, column) a register DFT_B over the rows of (j, k) of the three
 //            components, the Green multiply at frequency k + A k2, the
 //            inverse DFT_B, written back;
 //   stage 1 inverse: per (j, column) the conjugate twiddles and the inverse
@@ -61,15 +61,23 @@ __device__ __forceinline__ void xconv_stage(const PassArgs& a, unsigned char* sm
   __syncthreads();
 }
 
-// Intermediate layout in the tile: the value of (j, k) at row j A + k.  Stage
-// 1 reads rows j + B q and writes rows j A + k, which other jobs read, so
-// each thread holds one job (NT = B W) and the writes wait for all reads.
-template <typename T, int LT, int NT, int MINB, int A, int B, int P0, int P1, int P2, int TMA>
+// Intermediate layout in the tile (XL): 0 = the value of (j, k) at row
+// j + B k, where stage 1 writes the rows it read (in place, any number of jobs
+// per thread); 1 = at row j A + k, where a warp's middle jobs (consecutive k)
+// read rows one apart instead of B apart, free of bank conflicts for 8-byte
+// values, but stage 1 writes rows other jobs read, so each thread holds one
+// job (NT = B W) and the writes wait for all reads.
+template <int A, int B, int XL>
+__device__ __forceinline__ int xrow(int j, int k) {
+  return XL ? j * A + k : j + B * k;
+}
+
+template <typename T, int LT, int NT, int MINB, int A, int B, int P0, int P1, int P2, int TMA, int XL>
 __global__ void __launch_bounds__(NT, MINB) xconv2_kernel(const PassArgs a, const __grid_constant__ CUtensorMap tm,
                                                           const TmaTile tt) {
   constexpr int M = A * B, W = 3 * LT;
   static_assert(M == P0 * P1 * P2, "two-stage split and plan radices describe one axis");
-  static_assert(NT == B * W && NT == A * LT, "one stage-1 job and one middle job per thread");
+  static_assert(!XL || (NT == B * W), "layout 1 runs one stage-1 job per thread");
   extern __shared__ __align__(128) unsigned char smraw[];
   const bool from_tile = TMA && (smem_u32(pencil_tile<T, LT>(smraw, M)) & 127) == 0;
   if constexpr (TMA) {
@@ -92,9 +100,10 @@ __global__ void __launch_bounds__(NT, MINB) xconv2_kernel(const PassArgs a, cons
     }
   }
   const int n_in = a.n_in;
-  // stage 1, forward: this thread's job (j, col)
-  {
-    const int col = threadIdx.x % W, j = threadIdx.x / W;
+  // stage 1, forward
+#pragma unroll 1
+  for (int job = threadIdx.x; job < B * W; job += NT) {
+    const int col = job % W, j = job / W;
     T v[A];
     if (from_tile) {
 #pragma unroll
@@ -109,19 +118,20 @@ __global__ void __launch_bounds__(NT, MINB) xconv2_kernel(const PassArgs a, cons
     dft<A, false>(v);
 #pragma unroll
     for (int k = 1; k < A; ++k) v[k] = cmul(v[k], tw[j * k]);
-    __syncthreads();   // every read of the source rows is done
+    if constexpr (XL) __syncthreads();   // every read of the source rows is done
 #pragma unroll
-    for (int k = 0; k < A; ++k) sm[(j * A + k) * W + col] = v[k];
+    for (int k = 0; k < A; ++k) sm[xrow<A, B, XL>(j, k) * W + col] = v[k];
   }
   __syncthreads();
   // middle: DFT_B of the three components, Green multiply, inverse DFT_B
-  {
-    const int li = threadIdx.x % LT, k = threadIdx.x / LT;
+#pragma unroll 1
+  for (int job = threadIdx.x; job < A * LT; job += NT) {
+    const int li = job % LT, k = job / LT;
     T y[3][B];
 #pragma unroll
     for (int comp = 0; comp < 3; ++comp) {
 #pragma unroll
-      for (int jj = 0; jj < B; ++jj) y[comp][jj] = sm[(jj * A + k) * W + comp * LT + li];
+      for (int jj = 0; jj < B; ++jj) y[comp][jj] = sm[xrow<A, B, XL>(jj, k) * W + comp * LT + li];
       dft<B, false>(y[comp]);
     }
 #pragma unroll
@@ -137,26 +147,27 @@ __global__ void __launch_bounds__(NT, MINB) xconv2_kernel(const PassArgs a, cons
     for (int comp = 0; comp < 3; ++comp) {
       dft<B, true>(y[comp]);
 #pragma unroll
-      for (int jj = 0; jj < B; ++jj) sm[(jj * A + k) * W + comp * LT + li] = y[comp][jj];
+      for (int jj = 0; jj < B; ++jj) sm[xrow<A, B, XL>(jj, k) * W + comp * LT + li] = y[comp][jj];
     }
   }
   __syncthreads();
   // stage 1, inverse: rows below n_out to global memory
-  {
-    const int col = threadIdx.x % W, j = threadIdx.x / W;
+#pragma unroll 1
+  for (int job = threadIdx.x; job < B * W; job += NT) {
+    const int col = job % W, j = job / W;
     T v[A];
-    v[0] = sm[(j * A) * W + col];
+    v[0] = sm[xrow<A, B, XL>(j, 0) * W + col];
 #pragma unroll
-    for (int k = 1; k < A; ++k) v[k] = cmulc(sm[(j * A + k) * W + col], tw[j * k]);
+    for (int k = 1; k < A; ++k) v[k] = cmulc(sm[xrow<A, B, XL>(j, k) * W + col], tw[j * k]);
     dft<A, true>(v);
 #pragma unroll
     for (int q = 0; q < A; ++q) gstore<K_CONV, T, LT>(a, c, j + B * q, col, v[q]);
   }
 }
 
-template <typename T, int LT, int NT, int MINB, int A, int B, int P0, int P1, int P2, int TMA>
+template <typename T, int LT, int NT, int MINB, int A, int B, int P0, int P1, int P2, int TMA, int XL>
 int xconv2_launch(const PassArgs& a0, int64_t P0n, cudaStream_t st) {
-  static_assert(NT % 32 == 0 && NT <= 512 && MINB >= 1 && MINB < 16, "variant id encodes whole warps and MINB < 16");
+  static_assert(NT % 32 == 0 && NT <= 448 && MINB >= 1 && MINB < 16, "variant id encodes whole warps and MINB < 16");
   constexpr int M = A * B;
   PassArgs a = a0;
   if (a.ax.M != M || a.ax.nst != 3 || a.ax.rad[0] != P0 || a.ax.rad[1] != P1 || a.ax.rad[2] != P2 || a.green ||
@@ -168,8 +179,8 @@ int xconv2_launch(const PassArgs& a0, int64_t P0n, cudaStream_t st) {
   TmaTile tt;
   memset(&tt, 0, sizeof(tt));
   if (TMA && !make_tile_map<T, K_CONV, LT>(a, P0n, a.n_in, &tm, &tt))   // the plain loads
-    return xconv2_launch<T, LT, NT, MINB, A, B, P0, P1, P2, 0>(a0, P0n, st);
-  auto kern = xconv2_kernel<T, LT, NT, MINB, A, B, P0, P1, P2, TMA>;
+    return xconv2_launch<T, LT, NT, MINB, A, B, P0, P1, P2, 0, XL>(a0, P0n, st);
+  auto kern = xconv2_kernel<T, LT, NT, MINB, A, B, P0, P1, P2, TMA, XL>;
   const size_t smem = (size_t)pencil_smem_bytes<T>(M, LT, K_CONV);
   if (smem > 227 * 1024) return BDDA_BAD_ARG;
   const int64_t nblk = P0n * a.P1 * a.ntile;
@@ -183,9 +194,10 @@ int xconv2_launch(const PassArgs& a0, int64_t P0n, cudaStream_t st) {
 }
 
 // Table entry (kind K_CONV, the plan's radix sequence): variant id 2048 +
-// MINB + 16 NT/32, + 1024 with the TMA-filled tile.
-#define BDDA_XCONV2(T, PREC, LT, MINB, NT, A, B, P0, P1, P2, TMA)                                 \
-  { PREC, K_CONV, LT, MINB, 2048 + 1024 * (TMA) + MINB + 16 * ((NT) / 32), {P0, P1, P2, 1},         \
-    &xconv2_launch<T, LT, NT, MINB, A, B, P0, P1, P2, TMA>, 0 }
+// MINB + 16 NT/32, + 256 for intermediate layout 1, + 1024 with the
+// TMA-filled tile.
+#define BDDA_XCONV2(T, PREC, LT, MINB, NT, A, B, P0, P1, P2, TMA, XL)                                  \
+  { PREC, K_CONV, LT, MINB, 2048 + 1024 * (TMA) + 256 * (XL) + MINB + 16 * ((NT) / 32), {P0, P1, P2, 1}, \
+    &xconv2_launch<T, LT, NT, MINB, A, B, P0, P1, P2, TMA, XL>, 0 }
 
 }  // namespace bdda
