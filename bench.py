@@ -195,12 +195,13 @@ def run_bdda(args, rank, world, local_rank):
         d.solve_matrix_equation()
         return d.observables()
 
-    def timed(d, steps, sampler=None):
+    def timed(d, steps, step=None):
+        step = step or device_step
         barrier()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
         for _ in range(steps):
-            out = device_step(d)
+            out = step(d)
         e1.record()
         barrier()
         return max_over_ranks(e0.elapsed_time(e1) / steps), out
@@ -272,6 +273,40 @@ def run_bdda(args, rank, world, local_rank):
                           "max_rel_err_vs_converged_fp64": {"mixed": rel_errs(obs_m5, obsref),
                                                             "fp64": rel_errs(obs_645, obsref)}}
 
+    # ---- the learned warm start (the metric's FP32+refine+NN form): the FNO
+    # trained on the GPU on solver solutions of other particles (set-up,
+    # untimed, like the Green's spectrum); a step is the same step with the
+    # network's projected initial guess, inference inside the timed region ----
+    nn = None
+    if mixed and not args.no_nn:
+        model, tinfo = train_fno(args.nn_train, args.nn_epochs, args.fno_modes, args.fno_lr)
+        eps = (np.asarray(geo["m_p_xyz"], dtype=np.complex128) / float(geo["m_m"])) ** 2
+        nfb_box = [0]
+
+        def nn_step(d):
+            d.set_interaction_matrix(green=green)
+            for key in ("diag", "eper", "B"):   # formed again every step
+                d._dev.pop(key, None)
+            d._materialize()   # diag_A and B: the network's features
+            X0, nfb_box[0] = model.warm_start(d.lattice_n, d._dev["occ"], green, d._dev["diag"], d._dev["B"], eps,
+                                              mode="project")
+            d.solve_matrix_equation(X0=X0)
+            return d.observables()
+
+        dnn = make_dd("mixed")
+        nn_step(dnn)
+        ms_nn, obs_nn = timed(dnn, args.steps, nn_step)
+        nn = {"value": round(world * L / (ms_nn * 1e-3), 3), "ms_per_step": round(ms_nn, 3),
+              "iterations": dnn.iter_fin + 1, "converged": dnn.converge, "true_residual": dnn.err_fin,
+              "fallback_columns": int(nfb_box[0]), "mode": "projected (least squares over the predicted columns)",
+              "speedup_vs_mixed": round(ms / ms_nn, 3), "train": tinfo}
+        if plain is not None:
+            e_nn = rel_errs(obs_nn, obs64)
+            nn.update(speedup_vs_fp64=round(ms64 / ms_nn, 3), max_rel_err_vs_fp64=e_nn,
+                      accuracy_ok=bool(max(e_nn.values()) <= 1e-4),
+                      max_rel_err_vs_converged_fp64=rel_errs(obs_nn, obsref))
+        del model
+
     # ---- end to end through the public API, host numpy in and out ----
     def e2e_step():
         d = make_dd("mixed" if mixed else None)
@@ -325,15 +360,21 @@ def run_bdda(args, rank, world, local_rank):
     if mixed and _lib.C128 in lines:
         roofline["complex128_mvp"] = {k: lines[_lib.C128][k] for k in ("achieved", "mvp_ms", "mvps_timed")}
 
+    # the headline is the metric's form, FP32+refine+NN, when the network was
+    # trained and its step met the accuracy gate; the form without it beside
+    use_nn = nn is not None and nn.get("accuracy_ok", False) and nn["converged"]
+    ms_head = nn["ms_per_step"] if use_nn else ms
+    if plain is not None:
+        plain["speedup_of_headline"] = round(plain["ms_per_step"] / ms_head, 3)
     result = {
         "metric": METRIC,
-        "value": round(world * L / (ms * 1e-3), 3),
+        "value": round(world * L / (ms_head * 1e-3), 3),
         "unit": "orientations/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": round(ms, 3),
+        "ms_per_step": round(ms_head, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "complex64 products, complex128 Krylov + true residual" if mixed else "complex128",
-        "form": args.form,
+        "form": (args.form + "+nn") if use_nn else args.form,
         "tol": tol,
         "data": "synthetic: reference GRE geometry (seed 1) and SO(3) orientations (seed 2)",
         "config": dict(workload_config(L, tol), parallelism="replicas x%d" % world,
@@ -345,6 +386,9 @@ def run_bdda(args, rank, world, local_rank):
                        "observables stay within 1e-4 of the FP64 path's (accuracy gate); both forms at %g "
                        "are in at_metric_tol" % (tol, TOL, TOL)),
         "plain_fp64": plain,
+        "nn_warm_start": nn,
+        "mixed_without_nn": {"value": round(world * L / (ms * 1e-3), 3), "ms_per_step": round(ms, 3),
+                             "iterations": iters} if use_nn else None,
         "accuracy": accuracy,
         "at_metric_tol": metric_tol,
         "e2e": {"value": round(world * L / e2e_s, 3), "unit": "orientations/s",
@@ -903,41 +947,68 @@ def _fno_shape(spec):
     return _shape(spec)
 
 
-def run_fno(args):
-    """Train the FNO warm start on GPU-solved GRE particles and compare, on
-    held-out particles, iterations and time to 1e-5 from zero and from the
-    warm start (complex128 block-BiCGSTAB), with the fallback rate."""
+def _fno_shapes(specs):
+    """GRE lattices of the FNO particles, built on the host cores (spawned workers)."""
     import concurrent.futures
     import multiprocessing
-    from bdda_b200.warmstart import sample_particles
-    L = 16
-    train_specs = sample_particles(args.fno_train, seed=4)
-    eval_specs = sample_particles(args.fno_eval, seed=40)
     for var in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS"):
         os.environ[var] = "1"
-    t0 = time.perf_counter()
     with concurrent.futures.ProcessPoolExecutor(max_workers=max(1, min(32, (os.cpu_count() or 2) - 1)),
                                                 mp_context=multiprocessing.get_context("spawn")) as ex:
-        shapes = list(ex.map(_fno_shape, train_specs + eval_specs))
-    shape_s = time.perf_counter() - t0
+        return list(ex.map(_fno_shape, specs))
+
+
+def train_fno(n_train, epochs, modes, lr, shapes=None, L=16):
+    """The FNO warm start trained on the GPU on solver solutions of n_train GRE
+    particles (x ~ U[4,12], seed 4), L orientations each; returns the model
+    and a record of the training."""
     import torch
-    from bdda_b200.warmstart import WarmStartFNO, make_dataset
-    from bl_krylov import bl_krylov as bk
+    from bdda_b200.warmstart import WarmStartFNO, make_dataset, sample_particles
+    specs = sample_particles(n_train, seed=4)
     t0 = time.perf_counter()
-    train = make_dataset(train_specs, L=L, shapes=shapes[:len(train_specs)])
+    if shapes is None:
+        shapes = _fno_shapes(specs)
+    shape_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    train = make_dataset(specs, L=L, shapes=shapes)
     torch.cuda.synchronize()
     data_s = time.perf_counter() - t0
     for d in train:   # training needs no Green's spectrum
         d.pop("green", None)
     torch.cuda.empty_cache()
-    model = WarmStartFNO(layers=4, modes=args.fno_modes, seed=4)
+    model = WarmStartFNO(layers=4, modes=modes, seed=4)
     t0 = time.perf_counter()
-    losses = model.fit(train, epochs=args.fno_epochs, lr=args.fno_lr, lr_final=args.fno_lr * 0.05, seed=4)
+    losses = model.fit(train, epochs=epochs, lr=lr, lr_final=lr * 0.05, seed=4)
     torch.cuda.synchronize()
     train_s = time.perf_counter() - t0
+    del train
+    torch.cuda.empty_cache()
+    info = {"train_particles": n_train, "train_samples": n_train * L, "epochs": epochs, "modes": modes,
+            "params": model.n_params, "loss_first_epoch": round(losses[0], 4), "loss_last_epoch": round(losses[-1], 4),
+            "seconds": round(train_s, 2), "data_generation_s": round(data_s, 2), "shapes_host_s": round(shape_s, 2)}
+    return model, info
+
+
+def run_fno(args):
+    """Train the FNO warm start on GPU-solved GRE particles and compare, on
+    held-out particles, iterations and time to 1e-5 from zero and from the
+    warm start (complex128 block-BiCGSTAB), with the fallback rate."""
+    from bdda_b200.warmstart import sample_particles
+    L = 16
+    train_specs = sample_particles(args.fno_train, seed=4)
+    eval_specs = sample_particles(args.fno_eval, seed=40)
+    t0 = time.perf_counter()
+    shapes = _fno_shapes(train_specs + eval_specs)
+    shape_s = time.perf_counter() - t0
+    import torch
+    from bdda_b200.warmstart import make_dataset
+    from bl_krylov import bl_krylov as bk
+    model, tinfo = train_fno(args.fno_train, args.fno_epochs, args.fno_modes, args.fno_lr,
+                             shapes=shapes[:len(train_specs)], L=L)
+    losses = [tinfo["loss_first_epoch"], tinfo["loss_last_epoch"]]
+    train_s, data_s = tinfo["seconds"], tinfo["data_generation_s"]
     if args.fno_save:
         model.save(args.fno_save)
-    del train
     evald = make_dataset(eval_specs, L=L, shapes=shapes[len(train_specs):])
     rows = []
     for d in evald:
@@ -1065,6 +1136,10 @@ def main():
     ap.add_argument("--fno-lr", type=float, default=2e-3)
     ap.add_argument("--fno-save", default=None)
     ap.add_argument("--fno-verbose", action="store_true")
+    ap.add_argument("--no-nn", action="store_true",
+                    help="headline: skip the learned warm start (the FP32+refine form without the network)")
+    ap.add_argument("--nn-train", type=int, default=128, help="headline: FNO training particles")
+    ap.add_argument("--nn-epochs", type=int, default=10, help="headline: FNO training epochs")
     ap.add_argument("--fno-headline", action="store_true",
                     help="with --fno: also apply the trained network to the headline particle (x=20, L=64)")
     args = ap.parse_args()
