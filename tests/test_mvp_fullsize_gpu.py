@@ -126,9 +126,11 @@ def test_every_compiled_complex64_variant_gives_the_product(case):
 def test_tma_filled_tiles_give_the_plain_kernels_product(case, prec):
     """Each kernel whose tile is filled by a bulk tensor copy (id >= 1024)
     gives the product of the same kernel with the first stage's global loads
-    (id - 1024) to rounding (the copy moves the same values, zero-filled past
-    the source rows and columns as the loads are; the arithmetic is the same
-    code); no bounded wait of the copies ran out."""
+    (id - 1024) to rounding: the copy moves the same values, zero-filled past
+    the source rows and columns as the loads are, and the arithmetic is the
+    same source (complex128 1e-15; complex64 1e-6, where the compiler's
+    contraction of the two instantiations may differ); no bounded wait of the
+    copies ran out."""
     import ctypes as C
     lib = case["lib"].load()
     plan = case["plan"]
@@ -146,7 +148,7 @@ def test_tma_filled_tiles_give_the_plain_kernels_product(case, prec):
                     assert lib.bdda_tune_pass(prec, kind, M, 64, lt, v) == 0
                     Yt = _mvp(case, prec, case["S"])
                     err = (Yt - Yp).abs().max().item() / Yp.abs().max().item()
-                    assert err <= (1e-15 if prec == 0 else 1e-7), (prec, kind, axis, lt, v, err)
+                    assert err <= (1e-15 if prec == 0 else 1e-6), (prec, kind, axis, lt, v, err)
                     n_tma += 1
             assert n_tma, (prec, kind, axis)
             tested += n_tma
