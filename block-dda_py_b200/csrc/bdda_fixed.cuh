@@ -94,7 +94,9 @@ __device__ __forceinline__ void stage_job2(const PassArgs& a, const Pen& c, floa
   for (int q = 0; q < R; ++q) {
     const int row = base + q * span;
     float4 x;
-    if constexpr (SRC) x = gload2<KIND, LT>(a, c, row, col);
+    if constexpr (SRC == 1) x = gload2<KIND, LT>(a, c, row, col);
+    else if constexpr (SRC == 2) x = row < a.n_in ? *reinterpret_cast<const float4*>(sm + row * W + col)
+                                                  : make_float4(0.f, 0.f, 0.f, 0.f);
     else x = *reinterpret_cast<const float4*>(sm + row * W + col);
     v[q] = lo2(x);
     u[q] = hi2(x);
@@ -141,7 +143,9 @@ __device__ __forceinline__ void conv_mid_job2(const PassArgs& a, const Pen& c, f
     for (int q = 0; q < R; ++q) {
       const int row = b * R + q, col = comp * LT + li;
       float4 x;
-      if constexpr (SRC) x = gload2<K_CONV, LT>(a, c, row, col);
+      if constexpr (SRC == 1) x = gload2<K_CONV, LT>(a, c, row, col);
+      else if constexpr (SRC == 2) x = row < a.n_in ? *reinterpret_cast<const float4*>(sm + row * W + col)
+                                                    : make_float4(0.f, 0.f, 0.f, 0.f);
       else x = *reinterpret_cast<const float4*>(sm + row * W + col);
       y[comp][q] = lo2(x);
       z[comp][q] = hi2(x);
@@ -226,10 +230,11 @@ __device__ __forceinline__ void fixed_mid(const PassArgs& a, const Pen& c, T* sm
 // loads.  The tensor map views the source field as (l, component, row, p1,
 // p0), the last three ordered by stride, so a box lands as rows of the
 // [row][3 LT] tile; rows at or past n_in and columns at or past L come back
-// as zeros (out-of-bounds fill), as gload returns them.  Two boxes of
-// box_rows rows start at rows 0 and M - box_rows (they may overlap by a row
-// or two, written twice with the same bytes) so that each starts on a
-// 128-byte boundary of the tile.  The copy completes on a transaction
+// as zeros (out-of-bounds fill), as gload returns them.  The boxes cover the
+// source rows [0, n_in) only; the first stage reads no row past them (those
+// are zero).  Two boxes of box_rows rows start at rows 0 and n_in - box_rows
+// (they may overlap by a row or two, written twice with the same bytes) so
+// that each starts on a 128-byte boundary of the tile.  The copy completes on a transaction
 // barrier; the wait is bounded, and a CTA that gives up counts the event in
 // a.err, waits (bounded again) for its copy to land and returns.
 struct TmaTile {
@@ -284,12 +289,14 @@ __device__ __forceinline__ void tma_issue(const PassArgs& a, const CUtensorMap* 
   }
 }
 
-// First stage of a pass: reads the TMA-filled tile (from_tile) or global memory.
+// First stage of a pass: reads the TMA-filled tile (from_tile; the copy
+// brought rows [0, n_in), the rows past them are zero and not read) or
+// global memory.
 template <class RS, int S, bool INV, int DST, int KIND, typename T, int LT, int NT, int PAIR, int TMA>
 __device__ __forceinline__ void first_stage(const PassArgs& a, const Pen& c, T* sm, const T* tw, bool from_tile) {
   if constexpr (TMA) {
     if (from_tile) {
-      fixed_stage<RS, S, INV, 0, DST, KIND, T, LT, NT, PAIR>(a, c, sm, tw);
+      fixed_stage<RS, S, INV, 2, DST, KIND, T, LT, NT, PAIR>(a, c, sm, tw);
       return;
     }
   }
@@ -299,7 +306,7 @@ template <class RS, typename T, int LT, int NT, int PAIR, int TMA>
 __device__ __forceinline__ void first_mid(const PassArgs& a, const Pen& c, T* sm, const T* gs, bool from_tile) {
   if constexpr (TMA) {
     if (from_tile) {
-      fixed_mid<RS, 0, 1, T, LT, NT, PAIR>(a, c, sm, gs);
+      fixed_mid<RS, 2, 1, T, LT, NT, PAIR>(a, c, sm, gs);
       return;
     }
   }
@@ -473,7 +480,7 @@ int fixed_launch(const PassArgs& a0, int64_t P0, cudaStream_t st) {
   memset(&tm, 0, sizeof(tm));
   TmaTile tt;
   memset(&tt, 0, sizeof(tt));
-  if (TMA && !make_tile_map<T, KIND, LT>(a, P0, RS::M, &tm, &tt))   // not possible for this pass: the plain kernel
+  if (TMA && !make_tile_map<T, KIND, LT>(a, P0, a.n_in, &tm, &tt))   // not possible for this pass: the plain kernel
     return fixed_launch<T, KIND, LT, MINB, NT, PAIR, R0, R1, R2, R3, 0>(a0, P0, st);
   auto kern = fixed_pencil_kernel<T, KIND, LT, NT, MINB, R0, R1, R2, R3, PAIR, TMA>;
   const size_t smem = (size_t)pencil_smem_bytes<T>(RS::M, LT, KIND);

@@ -230,7 +230,8 @@ __device__ __forceinline__ void gstore(const PassArgs& a, const Pen& c, int row,
 
 // ---- one radix-R butterfly of a stage; rows base + q*span of column col ----
 // forward (DIF): DFT then twiddles w^(q*tws); inverse (DIT): conj twiddles then IDFT.
-// SRC / DST: 1 = global (fused with the load or the store), 0 = shared.
+// SRC / DST: 1 = global (fused with the load or the store), 0 = shared;
+// SRC 2 = shared, rows at or past n_in zero (not read).
 template <int R, bool INV, int SRC, int DST, int KIND, typename T, int LT>
 __device__ __forceinline__ void stage_job(const PassArgs& a, const Pen& c, T* sm, const T* tw, int col,
                                           int base, int span, int tws) {
@@ -239,7 +240,8 @@ __device__ __forceinline__ void stage_job(const PassArgs& a, const Pen& c, T* sm
 #pragma unroll
   for (int q = 0; q < R; ++q) {
     const int row = base + q * span;
-    if constexpr (SRC) v[q] = gload<KIND, T, LT>(a, c, row, col);
+    if constexpr (SRC == 1) v[q] = gload<KIND, T, LT>(a, c, row, col);
+    else if constexpr (SRC == 2) v[q] = row < a.n_in ? sm[row * W + col] : mkc<T>(0, 0);
     else v[q] = sm[row * W + col];
   }
   if constexpr (!INV) {
@@ -311,7 +313,8 @@ __device__ __forceinline__ void conv_mid_job(const PassArgs& a, const Pen& c, T*
 #pragma unroll
     for (int q = 0; q < R; ++q) {
       const int row = b * R + q, col = comp * LT + li;
-      if constexpr (SRC) y[comp][q] = gload<K_CONV, T, LT>(a, c, row, col);
+      if constexpr (SRC == 1) y[comp][q] = gload<K_CONV, T, LT>(a, c, row, col);
+      else if constexpr (SRC == 2) y[comp][q] = row < a.n_in ? sm[row * W + col] : mkc<T>(0, 0);
       else y[comp][q] = sm[row * W + col];
     }
     dft<R, false>(y[comp]);
