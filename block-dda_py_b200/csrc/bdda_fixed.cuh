@@ -222,73 +222,6 @@ __device__ __forceinline__ void fixed_mid(const PassArgs& a, const Pen& c, T* sm
   }
 }
 
-// ---- the tile's first read by a bulk tensor copy (TMA) ------------------------------------
-// With TMA = 1 the pencil's source rows of the CTA's column tile come into the
-// shared tile by one or two cp.async.bulk.tensor copies, issued by one thread
-// before the constants are staged (all bytes in flight at once); the first
-// radix stage then reads shared memory instead of issuing its own global
-// loads.  The tensor map views the source field as (l, component, row, p1,
-// p0), the last three ordered by stride, so a box lands as rows of the
-// [row][3 LT] tile; rows at or past n_in and columns at or past L come back
-// as zeros (out-of-bounds fill), as gload returns them.  The boxes cover the
-// source rows [0, n_in) only; the first stage reads no row past them (those
-// are zero).  Two boxes of box_rows rows start at rows 0 and n_in - box_rows
-// (they may overlap by a row or two, written twice with the same bytes) so
-// that each starts on a 128-byte boundary of the tile.  The copy completes on a transaction
-// barrier; the wait is bounded, and a CTA that gives up counts the event in
-// a.err, waits (bounded again) for its copy to land and returns.
-struct TmaTile {
-  int nbox, box_rows;
-  int rows;        // tile rows the boxes cover: [0, rows)
-  int dim_of[3];   // dimension 2 + d of the map holds (row, p1, p0)[dim_of[d]]
-};
-
-__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity, int limit) {
-  for (int i = 0; i < limit; ++i) {
-    uint32_t done;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(done)
-        : "r"(bar), "r"(parity)
-        : "memory");
-    if (done) return true;
-  }
-  return false;
-}
-
-constexpr int kTmaWaitLimit = 1 << 22;   // try_wait rounds: far beyond any copy's latency, but finite
-
-template <typename T, int KIND, int LT>
-__device__ __forceinline__ void tma_issue(const PassArgs& a, const CUtensorMap* tm, const TmaTile& tt,
-                                          unsigned char* smraw, int M, int64_t bid) {
-  constexpr int E = sizeof(T) / 8;   // 8-byte elements per complex value
-  T* sm = pencil_tile<T, LT>(smraw, M);
-  const uint32_t bar = smem_u32(pencil_barrier<T, KIND, LT>(smraw, M));
-  const int tile = (int)(bid % a.ntile);
-  const int64_t p = bid / a.ntile;
-  const int64_t p0 = p / a.P1, p1 = p - p0 * a.P1;
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(bar) : "memory");
-  asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
-  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-  const uint32_t bytes = (uint32_t)(tt.nbox * tt.box_rows * 3 * LT * (int)sizeof(T));
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes) : "memory");
-  for (int b = 0; b < tt.nbox; ++b) {
-    const int row0 = b == 0 ? 0 : tt.rows - tt.box_rows;
-    const int v[3] = {row0, (int)p1, (int)p0};
-    int c[3];
-#pragma unroll
-    for (int d = 0; d < 3; ++d) c[d] = v[tt.dim_of[d]];
-    const uint32_t dst = smem_u32(sm + (size_t)row0 * 3 * LT);
-    asm volatile(
-        "cp.async.bulk.tensor.5d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5, "
-        "%6}], [%7];\n" ::"r"(dst),
-        "l"(reinterpret_cast<uint64_t>(tm)), "r"(tile * LT * E), "r"(0), "r"(c[0]), "r"(c[1]), "r"(c[2]), "r"(bar)
-        : "memory");
-  }
-}
-
 // First stage of a pass: reads the TMA-filled tile (from_tile; the copy
 // brought rows [0, n_in), the rows past them are zero and not read) or
 // global memory.
@@ -336,17 +269,7 @@ __global__ void __launch_bounds__(NT, MINB) fixed_pencil_kernel(const PassArgs a
   stage_constants<T, KIND, LT>(a, smraw, RS::M, &tw, &sm, &gs, &cm, blockIdx.x);
   const Pen c = pen_of_block<T>(a, cm, blockIdx.x);
   if constexpr (TMA) {
-    if (from_tile) {
-      const uint32_t bar = smem_u32(pencil_barrier<T, KIND, LT>(smraw, RS::M));
-      const bool landed = mbar_wait_bounded(bar, 0, kTmaWaitLimit);
-      if (__syncthreads_or(!landed)) {   // the whole CTA leaves together
-        if (threadIdx.x == 0) {
-          if (a.err) atomicAdd(a.err, 1u);
-          mbar_wait_bounded(bar, 0, kTmaWaitLimit);   // the copy lands before the CTA's shared memory is released
-        }
-        return;
-      }
-    }
+    if (from_tile && !tile_landed<T, KIND, LT>(a, smraw, RS::M)) return;
   }
   if constexpr (KIND == K_FWD) {
     if constexpr (N == 1) {

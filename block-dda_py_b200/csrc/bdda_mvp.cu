@@ -21,6 +21,7 @@
 #include "bdda_internal.h"
 
 #include "bdda_blas.cuh"
+#include "bdda_fixed.cuh"
 #include "bdda_pencil.cuh"
 
 namespace bdda {
@@ -30,6 +31,23 @@ template <typename T, int KIND, int LT>
 __global__ void __launch_bounds__(256) pencil_kernel(const PassArgs a) {
   extern __shared__ __align__(16) unsigned char smraw[];
   generic_pencil<T, KIND, LT>(a, blockIdx.x, smraw);
+}
+
+// The same with the tile's source rows brought in by a bulk tensor copy
+// (make_tile_map), issued by one thread before the constants are staged.
+template <typename T, int KIND, int LT>
+__global__ void __launch_bounds__(256) pencil_tma_kernel(const PassArgs a, const __grid_constant__ CUtensorMap tm,
+                                                         const TmaTile tt) {
+  extern __shared__ __align__(128) unsigned char smraw[];
+  // the copy's destination must be 128-byte aligned; dynamic shared memory of
+  // a kernel without static shared memory starts on a wider boundary, so a
+  // miss is an error (counted like a wait that gave up), not a slower path
+  if ((smem_u32(pencil_tile<T, LT>(smraw, a.ax.M)) & 127) != 0) {
+    if (threadIdx.x == 0 && a.err) atomicAdd(a.err, 1u);
+    return;
+  }
+  if (threadIdx.x == 0) tma_issue<T, KIND, LT>(a, &tm, tt, smraw, a.ax.M, blockIdx.x);
+  generic_pencil<T, KIND, LT, 2>(a, blockIdx.x, smraw);
 }
 
 template <typename T>
@@ -82,16 +100,26 @@ static int pick_lt(int M, int L, int kind) {
 }
 
 template <typename T, int KIND, int LT>
-static int launch_lt(PassArgs a, int64_t P0, cudaStream_t st) {
-  auto kern = pencil_kernel<T, KIND, LT>;
+static int launch_lt(PassArgs a, int64_t P0, cudaStream_t st, bool tma = false) {
   a.ntile = (a.L + LT - 1) / LT;
   const size_t smem = pencil_smem<T>(a.ax.M, LT, KIND);
   if (smem > 227 * 1024) return BDDA_BAD_ARG;
   const int64_t nblk = P0 * a.P1 * a.ntile;
   if (nblk <= 0) return BDDA_OK;
   if (nblk > INT_MAX) return BDDA_BAD_ARG;
-  BDDA_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  kern<<<(unsigned)nblk, g_threads[prec_of<T>()][KIND], smem, st>>>(a);
+  CUtensorMap tm;
+  TmaTile tt;
+  memset(&tm, 0, sizeof(tm));
+  memset(&tt, 0, sizeof(tt));
+  if (tma && make_tile_map<T, KIND, LT>(a, P0, a.n_in, &tm, &tt)) {
+    auto kern = pencil_tma_kernel<T, KIND, LT>;
+    BDDA_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    kern<<<(unsigned)nblk, g_threads[prec_of<T>()][KIND], smem, st>>>(a, tm, tt);
+  } else {
+    auto kern = pencil_kernel<T, KIND, LT>;
+    BDDA_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    kern<<<(unsigned)nblk, g_threads[prec_of<T>()][KIND], smem, st>>>(a);
+  }
   BDDA_CUDA_TRY(cudaGetLastError());
   count_launch();
   return BDDA_OK;
@@ -164,18 +192,23 @@ static std::vector<int> fixed_variants(int prec, int kind, int lt, const AxisFFT
   return out;
 }
 
+// Generic kernels: variant -1 with the first stage's global loads, -2 with the
+// TMA-filled tile; with no choice made (variant 0) and no specialised kernel
+// for the radix sequence, the TMA-filled one where the pass allows it.
 template <typename T, int KIND>
 static int launch_pass(const PassArgs& a, int64_t P0, int lt, cudaStream_t st) {
+  int variant = 0;
   if (!a.green) {
-    const int variant = pass_tune(prec_of<T>(), KIND, a.ax.M, a.L).variant;
+    variant = pass_tune(prec_of<T>(), KIND, a.ax.M, a.L).variant;
     FixedLaunchFn f = fixed_find(prec_of<T>(), KIND, lt, a.ax, variant, pair_ok(a));
     if (f) return f(a, P0, st);
   }
+  const bool tma = variant != -1 && g_use_fixed;
   switch (lt) {
     case 16:   // tile width 16 exists as specialised kernels only
-    case 8: return launch_lt<T, KIND, 8>(a, P0, st);
-    case 4: return launch_lt<T, KIND, 4>(a, P0, st);
-    default: return launch_lt<T, KIND, 2>(a, P0, st);
+    case 8: return launch_lt<T, KIND, 8>(a, P0, st, tma);
+    case 4: return launch_lt<T, KIND, 4>(a, P0, st, tma);
+    default: return launch_lt<T, KIND, 2>(a, P0, st, tma);
   }
 }
 
@@ -325,7 +358,10 @@ static int autotune_impl(const bdda_plan* p, int L, const T* ghat, const int32_t
         if (pencil_smem<T>(M, lt, key.kind) > 227 * 1024) continue;
         for (int v : fixed_variants(prec, key.kind, lt, p->ax[key.axis], pair_ok(pa[q])))
           key.cand.push_back({prec, key.kind, M, L, lt, v});
-        if (lt <= 8) key.cand.push_back({prec, key.kind, M, L, lt, -1});   // generic kernels go up to 8
+        if (lt <= 8) {   // generic kernels go up to 8: global loads, TMA-filled tile
+          key.cand.push_back({prec, key.kind, M, L, lt, -1});
+          key.cand.push_back({prec, key.kind, M, L, lt, -2});
+        }
       }
       key.ms.assign(key.cand.size(), 0.0);
       keys.push_back(key);
@@ -550,7 +586,7 @@ int bdda_tune_set(int prec, int kind, size_t smem_budget, int threads) {
 
 int bdda_tune_pass(int prec, int kind, int M, int L, int lt, int variant) {
   if (prec < 0 || prec > 1 || kind < 0 || kind > 2 || M < 1 || L < 1 || L > kMaxL ||
-      (lt != 0 && lt != 2 && lt != 4 && lt != 8 && lt != 16) || variant < -1 || variant >= 4096)
+      (lt != 0 && lt != 2 && lt != 4 && lt != 8 && lt != 16) || variant < -2 || variant >= 4096)
     return BDDA_BAD_ARG;
   set_pass_tune({prec, kind, M, L, lt, variant});
   return BDDA_OK;

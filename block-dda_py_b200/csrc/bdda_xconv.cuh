@@ -87,17 +87,7 @@ __global__ void __launch_bounds__(NT, MINB) xconv2_kernel(const PassArgs a, cons
   xconv_stage<T, LT, A, B, P0, P1, P2>(a, smraw, &tw, &sm, &gs, blockIdx.x);
   const Pen c = pen_of_block<T>(a, nullptr, blockIdx.x);
   if constexpr (TMA) {
-    if (from_tile) {
-      const uint32_t bar = smem_u32(pencil_barrier<T, K_CONV, LT>(smraw, M));
-      const bool landed = mbar_wait_bounded(bar, 0, kTmaWaitLimit);
-      if (__syncthreads_or(!landed)) {   // the whole CTA leaves together
-        if (threadIdx.x == 0) {
-          if (a.err) atomicAdd(a.err, 1u);
-          mbar_wait_bounded(bar, 0, kTmaWaitLimit);
-        }
-        return;
-      }
-    }
+    if (from_tile && !tile_landed<T, K_CONV, LT>(a, smraw, M)) return;
   }
   const int n_in = a.n_in;
   // stage 1, forward

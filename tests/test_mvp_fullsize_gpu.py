@@ -161,6 +161,29 @@ def test_tma_filled_tiles_give_the_plain_kernels_product(case, prec):
 
 
 @pytest.mark.parametrize("prec", [0, 1])
+def test_generic_kernels_with_tma_tiles_give_the_same_product(case, prec):
+    """The run-time-radix kernels with the TMA-filled tile (variant -2, the
+    default for radix sequences without specialised kernels) give the product
+    of the same kernels with the first stage's global loads (variant -1):
+    complex128 to 1e-15, complex64 to 1e-6."""
+    lib = case["lib"].load()
+    plan = case["plan"]
+    passes = ((0, 2), (0, 1), (1, 0), (2, 1), (2, 2))
+    out = {}
+    try:
+        for v in (-1, -2):
+            for kind, axis in passes:
+                assert lib.bdda_tune_pass(prec, kind, plan.m[axis], 64, 8 if prec else 4, v) == 0
+            out[v] = _mvp(case, prec, case["S"])
+    finally:
+        for kind, axis in passes:
+            lib.bdda_tune_pass(prec, kind, plan.m[axis], 64, 0, 0)
+    err = (out[-2] - out[-1]).abs().max().item() / out[-1].abs().max().item()
+    assert err <= (1e-15 if prec == 0 else 1e-6), err
+    assert plan.wait_timeouts() == 0
+
+
+@pytest.mark.parametrize("prec", [0, 1])
 def test_two_stage_x_pass_gives_the_plan_stage_product(case, prec):
     """The X-pass kernels that transform the 192-point axis as 24 x 8 (ids
     from 2048; the plan's stages are [8,8,3]) give the product of the
