@@ -107,7 +107,9 @@ int bdda_tune_get(int prec, int kind, size_t* smem_budget, int* threads);
  * plain kernel otherwise; 2048 + (0 or 1024) + MINB + 16 * (threads / 32) =
  * an X-pass kernel that transforms the axis in two register stages (a
  * 192-point axis as 24 x 8) instead of the plan's radix sequence, with or
- * without the TMA-filled tile; -1 = the generic run-time-radix kernel).
+ * without the TMA-filled tile; -1 = the generic run-time-radix kernel, -2 =
+ * the same with the TMA-filled tile, which a pass without a specialised
+ * kernel for its radix sequence runs when no choice is set).
  * lt 16 exists as specialised kernels only.  Process-wide; set by
  * bdda_autotune. */
 int bdda_tune_pass(int prec, int kind, int M, int L, int lt, int variant);
