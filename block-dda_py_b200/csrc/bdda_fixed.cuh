@@ -50,8 +50,10 @@ __device__ __forceinline__ float4 gload2(const PassArgs& a, const Pen& c, int ro
   if constexpr (KIND == K_FWD) {
     if (c.cmap) {
       const int m = c.cmap[row];
-      return m >= 0 ? *reinterpret_cast<const float4*>(static_cast<const float2*>(a.S) + (int64_t)m * a.C + gcol)
-                    : z;
+      if (m < 0) return z;
+      const int64_t i = (int64_t)m * a.C + gcol;
+      if (a.wide) return pack2(narrow_at(a.S, i), narrow_at(a.S, i + 1));
+      return *reinterpret_cast<const float4*>(static_cast<const float2*>(a.S) + i);
     }
   }
   return *reinterpret_cast<const float4*>(static_cast<const float2*>(c.srcb) + (int64_t)row * a.src_row + gcol);
@@ -72,6 +74,11 @@ __device__ __forceinline__ void gstore2(const PassArgs& a, const Pen& c, int row
         const int64_t idx = (int64_t)m * a.C + gcol;
         const float2 d = static_cast<const float2*>(a.diag)[r3];
         const float2 j = static_cast<const float2*>(a.jpre)[r3];
+        if (a.wide) {
+          widen_to(a.dst, idx, cmul(cadd(cmul(d, narrow_at(a.S, idx)), cscale(v0, sc)), j));
+          widen_to(a.dst, idx + 1, cmul(cadd(cmul(d, narrow_at(a.S, idx + 1)), cscale(v1, sc)), j));
+          return;
+        }
         const float4 s = *reinterpret_cast<const float4*>(static_cast<const float2*>(a.S) + idx);
         const float2 o0 = cmul(cadd(cmul(d, lo2(s)), cscale(v0, sc)), j);
         const float2 o1 = cmul(cadd(cmul(d, hi2(s)), cscale(v1, sc)), j);

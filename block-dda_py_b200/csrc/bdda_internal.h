@@ -60,5 +60,11 @@ double mixed_diverge_factor();
 template <typename T>
 int block_mvp_impl(const bdda_plan* plan, int L, const T* ghat, const int32_t* cell_map,
                    const T* diag, const T* jpre, const T* S, T* out, T* work, cudaStream_t st);
+// The complex64 block MVP of a complex128 vector: the Z pass gathers S
+// rounding to complex64, the Z^-1 epilogue reads S the same way and writes
+// out widened to complex128 (the same values as rounding S into a complex64
+// copy and widening a complex64 result, without the copies).
+int block_mvp_wide(const bdda_plan* plan, int L, const float2* ghat, const int32_t* cell_map, const float2* diag,
+                   const float2* jpre, const double2* S, double2* out, float2* work, cudaStream_t st);
 
 }  // namespace bdda

@@ -290,10 +290,11 @@ template void mvp_pass_args<float2>(const bdda_plan*, int, const float2*, const 
 template <typename T>
 static int run_mvp(const bdda_plan* plan, int L, const T* ghat, const int32_t* cell_map,
                    const T* src, const T* diag, const T* jpre, T* out, T* F, cudaStream_t st,
-                   cudaEvent_t* ev = nullptr) {
+                   cudaEvent_t* ev = nullptr, bool wide = false) {
   PassArgs a[5];
   int64_t P0[5];
   mvp_pass_args<T>(plan, L, ghat, cell_map, src, diag, jpre, out, F, a, P0);
+  if (wide) a[0].wide = a[4].wide = 1;   // src and out are complex128 (complex64 passes)
   const bool prof = profiling();
   if (prof) profile_mark(0, st, prec_of<T>());
   if (ev) BDDA_CUDA_TRY(cudaEventRecord(ev[0], st));
@@ -314,6 +315,13 @@ int block_mvp_impl(const bdda_plan* plan, int L, const T* ghat, const int32_t* c
                    const T* diag, const T* jpre, const T* S, T* out, T* work, cudaStream_t st) {
   return run_mvp<T>(plan, L, ghat, cell_map, S, diag, jpre, out, work, st);
 }
+int block_mvp_wide(const bdda_plan* plan, int L, const float2* ghat, const int32_t* cell_map, const float2* diag,
+                   const float2* jpre, const double2* S, double2* out, float2* work, cudaStream_t st) {
+  if (!cell_map) return BDDA_BAD_ARG;
+  return run_mvp<float2>(plan, L, ghat, cell_map, reinterpret_cast<const float2*>(S), diag, jpre,
+                         reinterpret_cast<float2*>(out), work, st, nullptr, true);
+}
+
 template int block_mvp_impl<double2>(const bdda_plan*, int, const double2*, const int32_t*,
                                      const double2*, const double2*, const double2*, double2*,
                                      double2*, cudaStream_t);

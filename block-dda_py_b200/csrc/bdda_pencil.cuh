@@ -43,7 +43,17 @@ struct PassArgs {
   int gN[3], gM[3];
   double lf, k;
   unsigned int* err;    // bounded waits that gave up (the plan's counter; null: not counted)
+  int wide;             // complex64 passes: S (Z gather, Z^-1 epilogue) and the Z^-1 output are complex128
 };
+
+// Element m of a complex128 array as complex64 (round to nearest) and back.
+__device__ __forceinline__ float2 narrow_at(const void* p, int64_t i) {
+  const double2 d = static_cast<const double2*>(p)[i];
+  return make_float2((float)d.x, (float)d.y);
+}
+__device__ __forceinline__ void widen_to(void* p, int64_t i, float2 v) {
+  static_cast<double2*>(p)[i] = make_double2((double)v.x, (double)v.y);
+}
 
 struct Pen {
   int64_t p0, p1;
@@ -281,7 +291,11 @@ __device__ __forceinline__ T gload(const PassArgs& a, const Pen& c, int row, int
   if constexpr (KIND == K_FWD) {
     if (c.cmap) {
       const int m = c.cmap[row];
-      return m >= 0 ? static_cast<const T*>(a.S)[(int64_t)m * a.C + gcol] : mkc<T>(F(0), F(0));
+      if (m < 0) return mkc<T>(F(0), F(0));
+      if constexpr (std::is_same<T, float2>::value) {
+        if (a.wide) return narrow_at(a.S, (int64_t)m * a.C + gcol);
+      }
+      return static_cast<const T*>(a.S)[(int64_t)m * a.C + gcol];
     }
   }
   return static_cast<const T*>(c.srcb)[(int64_t)row * a.src_row + gcol];
@@ -303,6 +317,12 @@ __device__ __forceinline__ void gstore(const PassArgs& a, const Pen& c, int row,
         const int64_t idx = (int64_t)m * a.C + gcol;
         const T d = static_cast<const T*>(a.diag)[r3];
         const T j = static_cast<const T*>(a.jpre)[r3];
+        if constexpr (std::is_same<T, float2>::value) {
+          if (a.wide) {
+            widen_to(a.dst, idx, cmul(cadd(cmul(d, narrow_at(a.S, idx)), cscale(v, sc)), j));
+            return;
+          }
+        }
         const T s = static_cast<const T*>(a.S)[idx];
         static_cast<T*>(a.dst)[idx] = cmul(cadd(cmul(d, s), cscale(v, sc)), j);
       }

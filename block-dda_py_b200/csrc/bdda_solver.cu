@@ -67,7 +67,7 @@ __global__ void prepare_kernel(const double2* diag, const double2* B, int64_t nr
     const int64_t r = i / L;
     const double2 d = diag[r];
     const double2 j = zdiv(make_double2(1.0, 0.0), d);
-    Bj[i] = from_d2<T>(zmul(B[i], j));
+    if (Bj) Bj[i] = from_d2<T>(zmul(B[i], j));
     if (i % L == 0) {
       diagT[r] = from_d2<T>(d);
       jpreT[r] = from_d2<T>(j);
@@ -242,7 +242,7 @@ struct Ctx {
   // complex128 vectors with complex64 products (the mixed form): the product
   // inside the iteration runs on these buffers; null = complex128 products
   const float2* ghat32 = nullptr;
-  float2 *diag32 = nullptr, *jpre32 = nullptr, *in32 = nullptr, *out32 = nullptr;
+  float2 *diag32 = nullptr, *jpre32 = nullptr;
   bool diverged = false;   // set when the complex64-product recursion blew up
   T* xbest = nullptr;      // mixed form: X at the smallest residual so far (or null)
   double best = INFINITY;  // that residual
@@ -258,23 +258,14 @@ static int mvp_exact(Ctx<T>& c, const T* in, T* out) {
 }
 
 // The product inside the iteration: complex64 arithmetic when the context
-// carries complex64 buffers (input rounded to complex64, output widened).
+// carries complex64 buffers; the input is rounded to complex64 as the Z pass
+// gathers it and the output widened as the Z^-1 pass writes it.
 template <typename T>
 static int mvp(Ctx<T>& c, const T* in, T* out) {
   if constexpr (std::is_same<T, double2>::value) {
-    if (c.ghat32) {
-      const int64_t ne = c.n * c.L;
-      convert_in_kernel<float2><<<kRedBlocks, 256, 0, c.stream>>>(in, c.in32, ne);
-      count_launch();
-      BDDA_CUDA_TRY(cudaGetLastError());
-      const int s = block_mvp_impl<float2>(c.plan, c.L, c.ghat32, c.cell_map, c.diag32, c.jpre32, c.in32, c.out32,
-                                           reinterpret_cast<float2*>(c.field), c.stream);
-      if (s != BDDA_OK) return s;
-      convert_out_kernel<float2><<<kRedBlocks, 256, 0, c.stream>>>(c.out32, out, ne);
-      count_launch();
-      BDDA_CUDA_TRY(cudaGetLastError());
-      return BDDA_OK;
-    }
+    if (c.ghat32)
+      return block_mvp_wide(c.plan, c.L, c.ghat32, c.cell_map, c.diag32, c.jpre32, in, out,
+                            reinterpret_cast<float2*>(c.field), c.stream);
   }
   return mvp_exact(c, in, out);
 }
@@ -1114,16 +1105,13 @@ constexpr double kInnerFrac = 0.5;
 
 struct MLayout {
   Layout base;
-  size_t in32, out32, diag32, jpre32, xbest, total;
+  size_t diag32, jpre32, xbest, total;
 };
 
 static MLayout mlayout(const bdda_plan* p, int L, int n_occ) {
   MLayout o;
   o.base = layout(p, BDDA_C128, L, n_occ);
-  const size_t v32 = (size_t)3 * n_occ * L * 8;
   size_t off = o.base.total;
-  o.in32 = off; off = al(off + v32);
-  o.out32 = off; off = al(off + v32);
   o.diag32 = off; off = al(off + (size_t)3 * n_occ * 8);
   o.jpre32 = off; off = al(off + (size_t)3 * n_occ * 8);
   o.xbest = off; off = al(off + (size_t)3 * n_occ * L * 16);
@@ -1147,8 +1135,6 @@ static int run_mixed(int solver, const bdda_plan* p, int L, int n_occ, const voi
   TRY(allow_smem(cocg_alpha_kernel, c.sm3));
   TRY(allow_smem(cocg_xi_kernel, c.sm3));
   TRY(allow_smem(cocg_beta_kernel, c.sm3));
-  float2* in32 = reinterpret_cast<float2*>(w + o.in32);
-  float2* out32 = reinterpret_cast<float2*>(w + o.out32);
   float2* diag32 = reinterpret_cast<float2*>(w + o.diag32);
   float2* jpre32 = reinterpret_cast<float2*>(w + o.jpre32);
   const int64_t ne = c.n * L;
@@ -1162,7 +1148,7 @@ static int run_mixed(int solver, const bdda_plan* p, int L, int n_occ, const voi
     count_launch(2);
   } else {
     prepare_kernel<double2><<<kRedBlocks, 256, 0, st>>>(diag, B, c.n, L, c.diag, c.jpre, Bj);
-    prepare_kernel<float2><<<kRedBlocks, 256, 0, st>>>(diag, B, c.n, L, diag32, jpre32, in32);
+    prepare_kernel<float2><<<kRedBlocks, 256, 0, st>>>(diag, B, c.n, L, diag32, jpre32, nullptr);
     count_launch(3);
   }
   BDDA_CUDA_TRY(cudaGetLastError());
@@ -1177,8 +1163,6 @@ static int run_mixed(int solver, const bdda_plan* p, int L, int n_occ, const voi
     c.ghat32 = static_cast<const float2*>(ghat32);
     c.diag32 = diag32;
     c.jpre32 = jpre32;
-    c.in32 = in32;
-    c.out32 = out32;
     int it_in = 0;
     double err_in = INFINITY;
     const bool warm = round > 0 || X0 != nullptr;
