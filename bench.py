@@ -125,18 +125,22 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # algorithmic bytes of one block MVP (five pencil passes)
 # ---------------------------------------------------------------------------
-def mvp_pass_bytes(n, m, n_occ, L, s):
-    """Bytes each pass must move at minimum: every value it reads or writes once."""
+def mvp_pass_bytes(n, m, n_occ, L, s, sv=None):
+    """Bytes each pass must move at minimum: every value it reads or writes once.
+    s: bytes per complex value of the passes; sv: of the dipole vectors S and
+    the output (the mixed form's complex64 product reads and writes its
+    complex128 vectors directly: sv = 16)."""
+    sv = s if sv is None else sv
     Nx, Ny, Nz = n
     Mx, My, Mz = m
     C = 3 * L
     nc = Nx * Ny * Nz
     zrows, yrows = Nx * Ny * Mz, Nx * My * Mz
-    return [n_occ * C * s + nc * 4 + zrows * C * s,              # Z: gather S, forward z
+    return [n_occ * C * sv + nc * 4 + zrows * C * s,             # Z: gather S, forward z
             zrows * C * s + yrows * C * s,                       # Y: Ny rows in, My out
             2 * yrows * C * s + Mx * My * Mz * 6 * s,            # X: in place + Green spectrum
             yrows * C * s + zrows * C * s,                       # Y^-1
-            zrows * C * s + 2 * n_occ * C * s + 2 * 3 * n_occ * s + nc * 4]   # Z^-1 + epilogue
+            zrows * C * s + 2 * n_occ * C * sv + 2 * 3 * n_occ * s + nc * 4]   # Z^-1 + epilogue
 
 
 # ---------------------------------------------------------------------------
@@ -348,7 +352,8 @@ def run_bdda(args, rank, world, local_rank):
     lines = {}
     for prec, (per, cnt) in prof.items():
         s = 16 if prec == _lib.C128 else 8
-        pb = mvp_pass_bytes(plan.n, plan.m, dd.num_element_occupy, L, s)
+        # in the mixed form the complex64 product reads S and writes its output in complex128
+        pb = mvp_pass_bytes(plan.n, plan.m, dd.num_element_occupy, L, s, sv=16 if mixed else s)
         mvp_ms = sum(per)
         lines[prec] = {"alg_bytes_per_mvp": int(sum(pb)), "mvp_ms": round(mvp_ms, 3), "mvps_timed": cnt,
                        "achieved": round(sum(pb) / (mvp_ms * 1e-3) / 1e9, 1),
@@ -360,6 +365,8 @@ def run_bdda(args, rank, world, local_rank):
     traffic = None
     if main == _lib.C64 and list(plan.m) == [192, 224, 350]:
         traffic = int(sum((b - c) * L / 8 + c for b, c in zip(DRAM_L8_C64, DRAM_L8_CONST)))
+        if mixed:   # the Z pass gathers and the Z^-1 pass reads and writes complex128 dipole vectors
+            traffic += 3 * (8 * 3 * L * dd.num_element_occupy)
     roofline = {"kernel": "block MVP, %s (5 pencil passes)" % ("complex64" if main == _lib.C64 else "complex128"),
                 "bound": "hbm", "achieved": rl["achieved"], "peak": peak, "unit": "GB/s",
                 "frac": round(rl["achieved"] / peak, 3), "traffic": traffic, "peak_source": peak_src,
