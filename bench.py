@@ -144,6 +144,26 @@ def mvp_pass_bytes(n, m, n_occ, L, s, sv=None):
 
 
 # ---------------------------------------------------------------------------
+# replicas: one process per GPU, each solving the whole workload; the step
+# time is the slowest rank's, the throughput the sum over ranks
+# ---------------------------------------------------------------------------
+def max_over_ranks(x, world, device):
+    """The largest x over the ranks of the default process group (x itself for one rank)."""
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(world, units_per_rank, ms_per_step):
+    """Units per second of the whole job: every rank processes units_per_rank per step."""
+    return world * units_per_rank / (ms_per_step * 1e-3)
+
+
+# ---------------------------------------------------------------------------
 # the GPU arm
 # ---------------------------------------------------------------------------
 def run_bdda(args, rank, world, local_rank):
@@ -174,12 +194,11 @@ def run_bdda(args, rank, world, local_rank):
             dist.barrier()
         torch.cuda.synchronize()
 
-    def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    def slowest(x):
+        return max_over_ranks(x, world, dev)
+
+    def thr(ms_):
+        return round(replica_throughput(world, L, ms_), 3)
 
     # ---- set-up (untimed): resident geometry and Green's spectrum ----
     dd = make_dd("mixed" if mixed else None)
@@ -208,7 +227,7 @@ def run_bdda(args, rank, world, local_rank):
             out = step(d)
         e1.record()
         barrier()
-        return max_over_ranks(e0.elapsed_time(e1) / steps), out
+        return slowest(e0.elapsed_time(e1) / steps), out
 
     for _ in range(args.warmup):
         device_step(dd)
@@ -250,7 +269,7 @@ def run_bdda(args, rank, world, local_rank):
         dref.itermax = 400
         obsref = device_step(dref)
         err_mv64 = rel_errs(obs, obs64)
-        plain = {"value": round(world * L / (ms64 * 1e-3), 3), "unit": "orientations/s", "tol": tol,
+        plain = {"value": thr(ms64), "unit": "orientations/s", "tol": tol,
                  "ms_per_step": round(ms64, 3), "iterations": d64.iter_fin + 1,
                  "speedup_of_mixed": round(ms64 / ms, 3)}
         accuracy = {"gate": "max rel. error of C_ext, S_fw (theta, phi), S_bk, mixed vs FP64 at the same "
@@ -268,9 +287,9 @@ def run_bdda(args, rank, world, local_rank):
             ms_645, obs_645 = timed(d645, ksteps)
             e5 = rel_errs(obs_m5, obs_645)
             metric_tol = {"tol": TOL, "steps": ksteps,
-                          "mixed": {"value": round(world * L / (ms_m5 * 1e-3), 3), "ms_per_step": round(ms_m5, 3),
+                          "mixed": {"value": thr(ms_m5), "ms_per_step": round(ms_m5, 3),
                                     "iterations": dm5.iter_fin + 1},
-                          "fp64": {"value": round(world * L / (ms_645 * 1e-3), 3), "ms_per_step": round(ms_645, 3),
+                          "fp64": {"value": thr(ms_645), "ms_per_step": round(ms_645, 3),
                                    "iterations": d645.iter_fin + 1},
                           "speedup_of_mixed": round(ms_645 / ms_m5, 3),
                           "max_rel_err_mixed_vs_fp64": e5, "accuracy_ok": bool(max(e5.values()) <= 1e-4),
@@ -307,7 +326,7 @@ def run_bdda(args, rank, world, local_rank):
         ev_inf.clear()
         ms_nn, obs_nn = timed(dnn, args.steps, nn_step)
         inf_ms = float(np.mean([a.elapsed_time(b) for a, b in ev_inf]))
-        nn = {"value": round(world * L / (ms_nn * 1e-3), 3), "ms_per_step": round(ms_nn, 3),
+        nn = {"value": thr(ms_nn), "ms_per_step": round(ms_nn, 3),
               "iterations": dnn.iter_fin + 1, "converged": dnn.converge, "true_residual": dnn.err_fin,
               "warm_start_ms": round(inf_ms, 1),
               "fallback_columns": int(nfb_box[0]), "mode": "projected (least squares over the predicted columns)",
@@ -334,7 +353,7 @@ def run_bdda(args, rank, world, local_rank):
     for _ in range(max(1, args.steps)):
         d_e2e, _ = e2e_step()
     torch.cuda.synchronize()
-    e2e_s = max_over_ranks((time.perf_counter() - t0) / max(1, args.steps))
+    e2e_s = slowest((time.perf_counter() - t0) / max(1, args.steps))
     h2d = sum(d_e2e._dev[k].numel() * d_e2e._dev[k].element_size() for k in ("pos", "vec", "e0", "u_inc"))
     h2d += d_e2e._dev["occ"].address_dev.numel() * 8
     d2h = L * 12 * 8
@@ -385,7 +404,7 @@ def run_bdda(args, rank, world, local_rank):
         plain["speedup_of_headline"] = round(plain["ms_per_step"] / ms_head, 3)
     result = {
         "metric": METRIC,
-        "value": round(world * L / (ms_head * 1e-3), 3),
+        "value": thr(ms_head),
         "unit": "orientations/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(ms_head, 3),
@@ -404,11 +423,11 @@ def run_bdda(args, rank, world, local_rank):
                        "are in at_metric_tol" % (tol, TOL, TOL)),
         "plain_fp64": plain,
         "nn_warm_start": nn,
-        "mixed_without_nn": {"value": round(world * L / (ms * 1e-3), 3), "ms_per_step": round(ms, 3),
+        "mixed_without_nn": {"value": thr(ms), "ms_per_step": round(ms, 3),
                              "iterations": iters},
         "accuracy": accuracy,
         "at_metric_tol": metric_tol,
-        "e2e": {"value": round(world * L / e2e_s, 3), "unit": "orientations/s",
+        "e2e": {"value": thr(e2e_s * 1e3), "unit": "orientations/s",
                 "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                 "includes": "Target/IncidentField/DiscreteDipoles from host arrays, Green build, solve, "
                             "observables to host"},
