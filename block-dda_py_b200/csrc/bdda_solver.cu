@@ -321,8 +321,8 @@ double mixed_replace_drop() { return g_replace_drop; }
 // bdda_tune_mixed).  The fallback continues from the best X so far, so an
 // early call costs little: on a sweep of 48 strongly scattering problems
 // (m = 1.53) a factor of 10 took the mixed form from 11.3 to 16.2
-// orientations/s (complex128: 17.1), against 1000 before.  Block BiCGSTAB's
-// residual rises up to ~4-fold on the way down on the x=20 particle.
+// orientations/s (complex128: 17.1), against 1000 before.  The reference
+// residual is the first iteration's until the first replacement (below).
 static double g_diverge_factor = 10.0;
 
 double mixed_diverge_factor() { return g_diverge_factor; }
@@ -351,6 +351,7 @@ static int bicgstab_core(Ctx<T>& c, bool has_x0, double tol, int itermax, int* i
   double err = INFINITY;
   double rmax = 0.0;        // largest residual since the last replacement
   double rmin = INFINITY;   // smallest residual so far
+  double rfirst = INFINITY; // residual after the first iteration
   for (int k = 0; k < itermax; ++k) {
     TRY(mvp<T>(c, P, V));                                   // V = M^-1 A P
     TRY(gram2<T>(c, true, R0, V, R, c.sp.g2));              // R0^H V, R0^H R
@@ -403,12 +404,20 @@ static int bicgstab_core(Ctx<T>& c, bool has_x0, double tol, int itermax, int* i
     }
     rmax = err > rmax ? err : rmax;
     rmin = err < rmin ? err : rmin;
+    if (k == 0) rfirst = err;
     if (hist) hist[k] = err;
     *iter_fin = k;
     *err_fin = err;
     if (bad == 2) return BDDA_NOT_CONVERGED;   // NaN/Inf reached: stop, reported as not converged
     if (err < tol) return BDDA_OK;
-    if ((c.ghat32 || c.watch) && err > g_diverge_factor * rmin) {
+    // divergence: a rise by the factor above the smallest residual once the
+    // recursion has been checked against a true residual (a replacement);
+    // before that, above the first iteration's residual, because block
+    // BiCGSTAB's early hump rises well above its first minimum in exact
+    // arithmetic too (10.5-fold on the x=20 particle for one orientation set,
+    // in complex128 as in the mixed form), while a blow-up is unbounded
+    const double ref = c.replaced ? rmin : rfirst;
+    if ((c.ghat32 || c.watch) && err > g_diverge_factor * ref) {
       c.diverged = true;
       return BDDA_NOT_CONVERGED;
     }
