@@ -898,7 +898,7 @@ def run_sweep(args):
     arms = [a for a in args.sweep_arms.split(",") if a]
     table = {"one_at_a_time_fp64": (False, None), "one_at_a_time_mixed": (False, "mixed"),
              "batched_fp64": (True, None), "batched_mixed": (True, "mixed")}
-    totals = {a: dict(seconds=0.0, launches=0, converged=0, iters=[]) for a in arms}
+    totals = {a: dict(seconds=0.0, launches=0, converged=0, iters=[], unconverged=[]) for a in arms}
     obs = {a: {} for a in arms}
     green_s = 0.0
     warmed = False
@@ -932,7 +932,9 @@ def run_sweep(args):
             torch.cuda.synchronize()
             dt = time.perf_counter() - t0
             res = dict(seconds=dt, launches=int(lib.bdda_launch_count() - n0),
-                       converged=int(sum(d.converge for d in ds)), iters=[d.iter_fin + 1 for d in ds])
+                       converged=int(sum(d.converge for d in ds)), iters=[d.iter_fin + 1 for d in ds],
+                       unconverged=[dict(problem=int(p), cells=int(np.prod(d.lattice_n)), iterations=d.iter_fin + 1,
+                                         residual=float(d.err_fin)) for p, d in zip(ids, ds) if not d.converge])
             for d in ds:   # keep only the observables
                 for key in ("X", "B", "diag", "eper", "obs"):
                     d._dev.pop(key, None)
@@ -949,16 +951,20 @@ def run_sweep(args):
             t["launches"] += r["launches"]
             t["converged"] += r["converged"]
             t["iters"] += r["iters"]
+            t["unconverged"] += r["unconverged"]
             obs[name].update(zip(pids, o))
         del dds
         torch.cuda.empty_cache()
     res = {a: dict(value=round(len(problems) * L / t["seconds"], 2), seconds=round(t["seconds"], 3),
                    launches=t["launches"], converged=t["converged"],
-                   iterations_mean=round(float(np.mean(t["iters"])), 2)) for a, t in totals.items()}
-    obs = {a: [o[p] for p in sorted(o)] for a, o in obs.items()}
+                   iterations_mean=round(float(np.mean(t["iters"])), 2), unconverged=t["unconverged"])
+           for a, t in totals.items()}
     ref = obs.get("one_at_a_time_fp64")
     err = 0.0
-    for o, r in zip(obs.get("batched_mixed", []), ref if ref is not None else []):
+    bad = {u["problem"] for t in totals.values() for u in t["unconverged"]}
+    kept = [p for p in sorted(obs.get("batched_mixed", {})) if p not in bad]
+    for o, r in zip([obs["batched_mixed"][p] for p in kept] if "batched_mixed" in obs else [],
+                    [obs["one_at_a_time_fp64"][p] for p in kept] if ref is not None else []):
         for cols in ((1,), (2, 3), (4, 5), (10, 11)):
             a = o[:, cols[0]] + (1j * o[:, cols[1]] if len(cols) > 1 else 0)
             b = r[:, cols[0]] + (1j * r[:, cols[1]] if len(cols) > 1 else 0)
@@ -976,6 +982,7 @@ def run_sweep(args):
                         for a in res for b in res if a != b and a.startswith("batched") and
                         b.startswith("one_at_a_time")},
            "max_rel_err_batched_mixed_vs_fp64_observables": float("%.3g" % err) if ref is not None else None,
+           "observables_compared_over": "problems every arm converged",
            "setup_s": {"shapes_host": round(shape_s, 2), "green_spectra": round(green_s, 2)}}
     print(json.dumps(out), flush=True)
 

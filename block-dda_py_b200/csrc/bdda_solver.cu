@@ -321,9 +321,11 @@ double mixed_replace_drop() { return g_replace_drop; }
 // bdda_tune_mixed).  The fallback continues from the best X so far, so an
 // early call costs little: on a sweep of 48 strongly scattering problems
 // (m = 1.53) a factor of 10 took the mixed form from 11.3 to 16.2
-// orientations/s (complex128: 17.1), against 1000 before.  The reference
-// residual is the first iteration's until the first replacement (below).
+// orientations/s (complex128: 17.1), against 1000 before.  In the first
+// kEarlyHump iterations the reference is the first iteration's residual
+// (below).
 static double g_diverge_factor = 10.0;
+constexpr int kEarlyHump = 8;
 
 double mixed_diverge_factor() { return g_diverge_factor; }
 
@@ -410,13 +412,13 @@ static int bicgstab_core(Ctx<T>& c, bool has_x0, double tol, int itermax, int* i
     *err_fin = err;
     if (bad == 2) return BDDA_NOT_CONVERGED;   // NaN/Inf reached: stop, reported as not converged
     if (err < tol) return BDDA_OK;
-    // divergence: a rise by the factor above the smallest residual once the
-    // recursion has been checked against a true residual (a replacement);
-    // before that, above the first iteration's residual, because block
-    // BiCGSTAB's early hump rises well above its first minimum in exact
-    // arithmetic too (10.5-fold on the x=20 particle for one orientation set,
-    // in complex128 as in the mixed form), while a blow-up is unbounded
-    const double ref = c.replaced ? rmin : rfirst;
+    // divergence: a rise by the factor above the smallest residual; during
+    // the first kEarlyHump iterations before any replacement, above the first
+    // iteration's residual instead, because block BiCGSTAB's early hump rises
+    // well above its first minimum in exact arithmetic too (10.5-fold within
+    // five iterations on the x=20 particle for one orientation set, in
+    // complex128 as in the mixed form)
+    const double ref = (c.replaced || k >= kEarlyHump) ? rmin : rfirst;
     if ((c.ghat32 || c.watch) && err > g_diverge_factor * ref) {
       c.diverged = true;
       return BDDA_NOT_CONVERGED;
