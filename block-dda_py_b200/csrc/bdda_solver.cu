@@ -326,6 +326,12 @@ double mixed_replace_drop() { return g_replace_drop; }
 // (below).
 static double g_diverge_factor = 10.0;
 constexpr int kEarlyHump = 8;
+// ... and also abandoned once its smallest residual has not halved for
+// kStallIters iterations: on strongly scattering particles the complex64
+// recursion can stall between 1e-4 and 4e-4 without a 10-fold rise (two of
+// the 144 sweep problems ran 500 iterations that way); the complex128
+// fallback then continues from the best X.
+constexpr int kStallIters = 60;
 
 double mixed_diverge_factor() { return g_diverge_factor; }
 
@@ -354,6 +360,8 @@ static int bicgstab_core(Ctx<T>& c, bool has_x0, double tol, int itermax, int* i
   double rmax = 0.0;        // largest residual since the last replacement
   double rmin = INFINITY;   // smallest residual so far
   double rfirst = INFINITY; // residual after the first iteration
+  double rstall = INFINITY; // residual at the last halving of the smallest one
+  int kstall = 0;           // iteration of that halving
   for (int k = 0; k < itermax; ++k) {
     TRY(mvp<T>(c, P, V));                                   // V = M^-1 A P
     TRY(gram2<T>(c, true, R0, V, R, c.sp.g2));              // R0^H V, R0^H R
@@ -407,6 +415,10 @@ static int bicgstab_core(Ctx<T>& c, bool has_x0, double tol, int itermax, int* i
     rmax = err > rmax ? err : rmax;
     rmin = err < rmin ? err : rmin;
     if (k == 0) rfirst = err;
+    if (err < 0.5 * rstall) {
+      rstall = err;
+      kstall = k;
+    }
     if (hist) hist[k] = err;
     *iter_fin = k;
     *err_fin = err;
@@ -419,7 +431,7 @@ static int bicgstab_core(Ctx<T>& c, bool has_x0, double tol, int itermax, int* i
     // five iterations on the x=20 particle for one orientation set, in
     // complex128 as in the mixed form)
     const double ref = (c.replaced || k >= kEarlyHump) ? rmin : rfirst;
-    if ((c.ghat32 || c.watch) && err > g_diverge_factor * ref) {
+    if (((c.ghat32 || c.watch) && err > g_diverge_factor * ref) || (c.ghat32 && k - kstall >= kStallIters)) {
       c.diverged = true;
       return BDDA_NOT_CONVERGED;
     }
