@@ -268,7 +268,14 @@ size_t bdda_mixed_workspace_bytes(const bdda_plan* plan, int L, int n_occ);
  * solver's mode MIXED for replace_drop and diverge_factor): replace_drop in
  * (0, 1), default 0.1; switch_ratio >= 0, default 0 (complex64 products to
  * the end); diverge_factor > 1, default 10: the recursion counts as
- * diverged once its residual exceeds its smallest value so far by this. */
+ * diverged once its residual exceeds its smallest value so far by this
+ * (in the one-problem solver: in its first 8 iterations before any residual
+ * replacement, the first iteration's residual instead, which block
+ * BiCGSTAB's early rise can exceed tenfold; a recursion whose smallest
+ * residual has not halved in 60 iterations counts as stalled, with the same
+ * complex128 fallback). */
+int bdda_tune_mixed(double replace_drop, double switch_ratio, double diverge_factor);
+int bdda_tune_mixed_get(double* replace_drop, double* switch_ratio, double* diverge_factor);
 /* Small one-problem solves (padded grid points x L <= 64 Mi, itermax <= 4096,
  * plain complex128 / complex64 forms) run their iterations as a CUDA graph
  * "while" node: one iteration is captured as the body and the loop condition
@@ -276,8 +283,6 @@ size_t bdda_mixed_workspace_bytes(const bdda_plan* plan, int L, int n_occ);
  * and one read-back instead of ~20 launches and a synchronisation per
  * iteration.  on = 0 uses the host-driven loop everywhere (process-wide). */
 int bdda_tune_solver_graphs(int on);
-int bdda_tune_mixed(double replace_drop, double switch_ratio, double diverge_factor);
-int bdda_tune_mixed_get(double* replace_drop, double* switch_ratio, double* diverge_factor);
 int bdda_mixed_solve(const bdda_plan* plan, int solver, int L, int n_occ, const void* ghat_c128,
                      const void* ghat_c64, const int32_t* cell_map, const void* diag, const void* B,
                      const void* X0, double tol, int itermax, int max_outer, void* X, int* iter_fin,
