@@ -35,7 +35,7 @@ def _rank(rank, world, port, out):
 
 def test_two_replicas_report_the_slowest_step_and_the_summed_throughput():
     world = 2
-    out = mp.Manager().dict()
+    out = mp.get_context("spawn").Manager().dict()   # no fork of a threaded process
     mp.spawn(_rank, args=(world, _free_port(), out), nprocs=world, join=True)
     assert out[0] == out[1]
     slow, value = out[0]
